@@ -1,0 +1,243 @@
+/*
+ * fgss.h -- C ABI of libfgss, the B200 (sm_100a) Jaccard set-similarity
+ * self-join.  Plain C types only; every call returns a status and never exits.
+ *
+ * The reference project (RafaelQuirino/new_fgssjoin) has no library API: its
+ * boundary is the `fgssjoin <ppjoin.bin> <threshold>` process
+ * (src/fgssjoin_cli.cu:13-112) over four internal host calls.  Each entry
+ * point below names the reference interface it replaces.
+ *
+ * Record order.  Record arrays are in the reference's MEMORY order: the .bin
+ * file order reversed (src/fgssjoin/data.cu:97-113), i.e. descending size for
+ * a well-formed file.  Pairs are oriented as the reference prints them:
+ * (record with the lower memory index, record with the higher one) -- the
+ * larger set first.
+ *
+ * Ownership.  The caller owns its inputs.  The library owns what it returns
+ * (fgss_sets, fgss_pairs) until the matching *_free call.
+ *
+ * Threading.  A context is bound to one device and one stream and is not
+ * thread-safe; separate contexts are independent.
+ */
+#ifndef FGSS_H_
+#define FGSS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FGSS_VERSION_MAJOR 0
+#define FGSS_VERSION_MINOR 1
+
+typedef enum fgss_status {
+    FGSS_OK = 0,
+    FGSS_ERR_INVALID = 1,      /* bad argument */
+    FGSS_ERR_CUDA = 2,         /* CUDA runtime error (message in fgss_last_error) */
+    FGSS_ERR_NOMEM = 3,        /* host or device allocation failed */
+    FGSS_ERR_FORMAT = 4,       /* malformed input (truncated .bin, unsorted tokens ...) */
+    FGSS_ERR_IO = 5,           /* file could not be opened / read / written */
+    FGSS_ERR_UNSUPPORTED = 6,  /* outside the supported limits (set length > 65535 ...) */
+    FGSS_ERR_TIMEOUT = 7,      /* a bounded device wait gave up */
+    FGSS_ERR_CAPACITY = 8      /* a caller-sized buffer is too small */
+} fgss_status;
+
+typedef struct fgss_ctx fgss_ctx;
+
+/* ---------------------------------------------------------------- context */
+
+typedef struct fgss_options {
+    int device;                  /* CUDA device ordinal (reference: device 0, fgssjoin_cli.cu:81) */
+    void* stream;                /* cudaStream_t to run on; NULL = the library creates its own */
+    int verbose;                 /* per-stage timings on stderr */
+    const char* tune_cache_path; /* autotuner cache (JSON); NULL = in-memory only */
+} fgss_options;
+
+void fgss_options_default(fgss_options* opt);
+fgss_status fgss_create(fgss_ctx** ctx, const fgss_options* opt);
+void fgss_destroy(fgss_ctx* ctx);
+const char* fgss_strerror(fgss_status st);
+/* Detailed message of the last failing call on this context ("" if none). */
+const char* fgss_last_error(const fgss_ctx* ctx);
+int fgss_version(void);
+
+/* ------------------------------------------------------------------- sets */
+
+/* Library-owned record arrays (host memory), MEMORY order.
+ * Reference: sets_t, include/fgssjoin/data.cuh:12-50. */
+typedef struct fgss_sets {
+    uint32_t* id;       /* record id (1-based input line number for tokenized text) */
+    uint32_t* pos;      /* offset of each record in tokens */
+    uint32_t* len;      /* size of each record */
+    uint32_t* tokens;   /* all records concatenated, ascending term ids per record */
+    uint32_t* loc;      /* per token: its q-gram position in the line (NULL when unknown) */
+    uint64_t n_sets;
+    uint64_t n_tokens;
+    uint32_t n_terms;   /* max token + 1 (data.cu:77-78) */
+    uint32_t max_len;
+} fgss_sets;
+
+/* A borrowed view of record arrays, host or device memory, MEMORY order. */
+typedef struct fgss_sets_view {
+    const uint32_t* id;
+    const uint32_t* pos;
+    const uint32_t* len;
+    const uint32_t* tokens;
+    uint64_t n_sets;
+    uint64_t n_tokens;
+    uint32_t n_terms;
+    int on_device;      /* 1 = the four pointers are device pointers on the context's device */
+} fgss_sets_view;
+
+/* Reads a ppjoin .bin ([int32 id][int32 size][int32 token x size]...) into
+ * MEMORY order.  Replaces sets_t* ppjoin_format(const char*, char)
+ * (include/fgssjoin/data.cuh:57-60, src/fgssjoin/data.cu:31-126). */
+fgss_status fgss_load_bin(const char* path, fgss_sets* out);
+
+/* Writes sets (MEMORY order) as a .bin in FILE order (ascending size), and the
+ * .loc side file when loc_path is not NULL and sets->loc is set.  The reference
+ * has no writer (src/preprocess_cli.cpp:346-347 "TODO"); the layout is the one
+ * its loader reads. */
+fgss_status fgss_write_bin(const char* path, const char* loc_path, const fgss_sets* sets);
+
+void fgss_sets_free(fgss_sets* sets);
+fgss_sets_view fgss_sets_view_of(const fgss_sets* sets);
+
+/* ------------------------------------------------------------- tokenizer */
+
+enum { FGSS_TOK_QGRAM = 0, FGSS_TOK_KMER = 1 };
+
+typedef struct fgss_tok_opts {
+    int q;          /* q-gram size, or k for k-mers (<= 32) */
+    int mode;       /* FGSS_TOK_QGRAM / FGSS_TOK_KMER */
+    int pad;        /* q-grams: pad each line with q-1 pad_char on both sides */
+    int pad_char;   /* padding byte (default 0x01) */
+    int suffix;     /* q-grams: 1 = each repeat is its own token (gram + occurrence,
+                       src/preprocess/string/qgram.cpp:27-44); 0 = distinct grams */
+    int lower;      /* ASCII lower-case first (src/preprocess/string/data.cpp:36-40) */
+} fgss_tok_opts;
+
+void fgss_tok_opts_default(fgss_tok_opts* o);
+
+/* Text (lines separated by '\n'; empty lines skipped, src/io.cpp:8-26) ->
+ * token sets on the GPU: q-grams or canonical k-mers, term ids by ascending
+ * document frequency with ties broken by first occurrence
+ * (src/preprocess_cli.cpp:266-340 and the fixture
+ * test/data/string/small.txt.3gram.bin), ids ascending within a record,
+ * records ordered as a .bin lists them and returned in MEMORY order.
+ * Lines that yield no token are dropped.  Replaces the reference's
+ * preprocess pipeline (src/preprocess_cli.cpp:222-358). */
+fgss_status fgss_tokenize(fgss_ctx* ctx, const char* text, uint64_t n_bytes,
+                          const fgss_tok_opts* opts, fgss_sets* out);
+
+/* ------------------------------------------------------------------ join */
+
+enum { FGSS_BOUNDS_REFERENCE = 0, /* float32 bounds exactly as similarity.cuh:9-82 */
+       FGSS_BOUNDS_EXACT = 1 };   /* exact rational bounds of the decimal threshold */
+enum { FGSS_METHOD_PLAIN = 0,     /* per-stage launches, exact two-pass counts */
+       FGSS_METHOD_BATCHED = 1 }; /* persistent fused kernel, learned presizing, CUDA graph */
+
+typedef struct fgss_join_opts {
+    float threshold;        /* Jaccard threshold in (0, 1) (fgssjoin_cli.cu:31-35) */
+    int bounds;             /* FGSS_BOUNDS_* */
+    int method;             /* FGSS_METHOD_* */
+    int out_on_device;      /* 1 = pairs stay in device memory (library-owned) */
+    int want_candidates;    /* 1 = also return the candidate list (debug / tests) */
+    int use_model;          /* batched method: presize and bin with the learned model */
+} fgss_join_opts;
+
+void fgss_join_opts_default(fgss_join_opts* o);
+
+typedef struct fgss_stats {
+    uint64_t candidates;      /* "# Candidates"  (block.cu:180,209) */
+    uint64_t intersections;   /* "# Intersections" (block.cu:181,210) */
+    uint64_t results;         /* "# Results" (block.cu:194,211) */
+    uint64_t index_entries;   /* "# Inverted Index Entries" (fgssjoin_cli.cu:92) */
+    uint64_t probe_tokens;    /* sum of probe-prefix lengths */
+    uint64_t window_entries;  /* list entries inside the id+size windows that the filter read */
+    uint64_t verified;        /* candidates that needed a merge */
+    uint64_t heavy_queries;   /* queries that took the global-memory accumulator */
+    uint32_t overflow_retries;/* presized buffers that overflowed and were re-run exactly */
+    float ms_total;           /* device time of the whole call (CUDA events) */
+    float ms_index;           /* prefix lengths + inverted index */
+    float ms_filter;          /* candidate generation (+ verification when fused) */
+    float ms_verify;          /* verification (plain method) */
+    float ms_output;          /* compaction, sort, copy-out */
+    float ms_probe;           /* batched method: the fused filter+verify kernel alone */
+    uint64_t merged_tokens;   /* source tokens the fused kernel's merges read */
+    uint64_t launches;        /* kernels launched by the call */
+} fgss_stats;
+
+typedef struct fgss_pairs {
+    uint32_t* q;        /* memory index of the first record */
+    uint32_t* s;        /* memory index of the second record */
+    uint32_t* id_q;     /* id[q] */
+    uint32_t* id_s;     /* id[s] */
+    uint32_t* overlap;  /* |x n y| */
+    float* sim;         /* float(overlap) / float(|x| + |y| - overlap) (similarity.cuh:78-82) */
+    uint64_t n;
+    int on_device;
+    /* candidates (want_candidates): (q, s, partial score) triples, host memory */
+    uint32_t* cand;
+    uint64_t n_cand;
+    void* priv;
+} fgss_pairs;
+
+/* Self-join at one threshold; pairs sorted by (q, s).  Replaces
+ * prepare_data + inverted_index + process_blocks
+ * (data.cuh:72-74, index.cuh:99-100, block.cuh:13-14; src/fgssjoin_cli.cu:86-100). */
+fgss_status fgss_selfjoin(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_join_opts* opts,
+                          fgss_pairs* out, fgss_stats* stats);
+
+/* Many independent self-joins (each with its own sets and threshold) in one
+ * persistent launch per stage.  outs and stats are arrays of n (stats may be
+ * NULL).  No reference counterpart: it runs process_blocks once per join. */
+fgss_status fgss_selfjoin_batch(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_join_opts* opts,
+                                int n, fgss_pairs* outs, fgss_stats* stats);
+
+void fgss_pairs_free(fgss_pairs* p);
+
+/* Formats pairs as the reference prints them: "%d %d %f\n" per pair
+ * (block.cu:193).  Writes to the FILE* given as a void* (stdout if NULL). */
+fgss_status fgss_pairs_print(const fgss_pairs* p, void* file);
+
+/* ------------------------------------------------------- learned cost model */
+
+/* Trains the 2-layer FP32 MLP of the batched method on counts logged by the
+ * exact count pass over the given joins (GPU forward/backward kernels), and
+ * keeps it in the context.  No reference counterpart. */
+fgss_status fgss_model_train(fgss_ctx* ctx, const fgss_sets_view* sets, const float* thresholds,
+                             int n, int epochs, float lr, uint64_t seed, float* final_loss);
+fgss_status fgss_model_save(fgss_ctx* ctx, const char* path);
+fgss_status fgss_model_load(fgss_ctx* ctx, const char* path);
+
+/* Host-side bound tables of one threshold (no device needed): for lengths
+ * n <= max_len the probe prefix (jac_max_prefix), index prefix
+ * (jac_mid_prefix), floor(n t) and floor(n / t) of
+ * include/fgssjoin/similarity.cuh:9-58, and for length sums S <= 2 max_len the
+ * smallest overlap the final test of src/fgssjoin/block.cu:190-193 accepts.
+ * Any output pointer may be NULL. */
+fgss_status fgss_bounds_table(float threshold, int bounds, uint32_t max_len, uint16_t* probe, uint16_t* index,
+                              uint32_t* min_size, uint32_t* max_size, uint32_t* need);
+
+/* ------------------------------------------------- device-level primitives */
+/* Stage kernels exposed for tests and callers that keep data on the device.
+ * All pointers are device pointers; the work runs on the context's stream
+ * and the call returns after it completes. */
+
+/* Exclusive prefix sum of n uint32 values (out may alias in).
+ * Replaces exclusive_scan<unsigned int> (include/fgssjoin/scan.cuh:39-105). */
+fgss_status fgss_dev_exclusive_scan_u32(fgss_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t n);
+
+/* Stable LSD radix sort of n (key, value) pairs by key bits [begin_bit, end_bit).
+ * No reference counterpart (the reference sorts on the host, preprocess_cli.cpp:170-215). */
+fgss_status fgss_dev_sort_pairs_u64(fgss_ctx* ctx, uint64_t* keys, uint32_t* values, uint64_t n,
+                                    int begin_bit, int end_bit);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FGSS_H_ */

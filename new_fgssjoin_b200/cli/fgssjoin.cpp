@@ -1,0 +1,186 @@
+// fgssjoin -- command line front end of libfgss.
+//
+// Two argument forms:
+//   fgssjoin <ppjoin.bin> <threshold> [verbose|debug]      the reference binary's form
+//                                                          (src/fgssjoin_cli.cu:20-49)
+//   fgssjoin -f <text> -q <q> -t <threshold> [options]     the form its README documents
+//                                                          (README.md:12-15,46): text in,
+//                                                          tokenized on the GPU
+// Options of the second form: --pad (pad q-grams), --distinct (one token per
+// distinct gram instead of gram + occurrence), --kmer (canonical k-mers, k = q),
+// --method plain|batched, --bounds reference|exact, --write-bin <path> (also
+// write the tokenized .bin and .bin.loc), --device <n>.
+// stdout: "id id similarity" per pair (block.cu:193); stderr: the reference's
+// counters and timers (fgssjoin_cli.cu:55-65,92,108; block.cu:209-212).
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/time.h>
+#include <unistd.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/fgss.h"
+
+static double now_us() {
+    struct timeval tv;
+    gettimeofday(&tv, nullptr);
+    return tv.tv_sec * 1e6 + tv.tv_usec;
+}
+
+static int die(fgss_ctx* ctx, fgss_status st, const char* what) {
+    fprintf(stderr, "%s: %s (%s)\n", what, fgss_strerror(st), ctx ? fgss_last_error(ctx) : fgss_last_error(nullptr));
+    return 1;
+}
+
+static void usage(const char* argv0) {
+    fprintf(stdout,
+            "Usage:\n"
+            "  %s <ppjoin bin file> <threshold> [verbose|debug]\n"
+            "  %s -f <text file> -q <q> -t <threshold> [--pad] [--distinct] [--kmer]\n"
+            "     [--method plain|batched] [--bounds reference|exact] [--write-bin <path>] [--device <n>]\n",
+            argv0, argv0);
+}
+
+int main(int argc, char** argv) {
+    if (argc < 3) {
+        usage(argv[0]);
+        return 1;
+    }
+    std::string bin_path, text_path, write_bin;
+    float threshold = 0.f;
+    int q = 3, pad = 0, suffix = 1, kmer = 0, method = FGSS_METHOD_PLAIN, bounds = FGSS_BOUNDS_REFERENCE;
+    int device = 0;
+    char verbose = 0, debug = 0;
+    if (argv[1][0] == '-') {
+        for (int i = 1; i < argc; i++) {
+            std::string a = argv[i];
+            auto next = [&](const char* what) -> const char* {
+                if (i + 1 >= argc) {
+                    fprintf(stderr, "missing value for %s\n", what);
+                    exit(1);
+                }
+                return argv[++i];
+            };
+            if (a == "-f") text_path = next("-f");
+            else if (a == "-q") q = atoi(next("-q"));
+            else if (a == "-t") threshold = (float)atof(next("-t"));
+            else if (a == "--pad") pad = 1;
+            else if (a == "--distinct") suffix = 0;
+            else if (a == "--kmer") kmer = 1;
+            else if (a == "--method") method = strcmp(next("--method"), "batched") == 0 ? FGSS_METHOD_BATCHED : FGSS_METHOD_PLAIN;
+            else if (a == "--bounds") bounds = strcmp(next("--bounds"), "exact") == 0 ? FGSS_BOUNDS_EXACT : FGSS_BOUNDS_REFERENCE;
+            else if (a == "--write-bin") write_bin = next("--write-bin");
+            else if (a == "--device") device = atoi(next("--device"));
+            else if (a == "verbose" || a == "--verbose") verbose = 1;
+            else {
+                usage(argv[0]);
+                return 1;
+            }
+        }
+        if (text_path.empty()) {
+            usage(argv[0]);
+            return 1;
+        }
+    } else {
+        bin_path = argv[1];
+        threshold = (float)atof(argv[2]);  // fgssjoin_cli.cu:31
+        for (int i = 3; i < argc && i < 5; i++) {
+            if (strcmp(argv[i], "verbose") == 0) verbose = 1;
+            if (strcmp(argv[i], "debug") == 0) debug = 1;
+        }
+    }
+    const std::string& in_path = bin_path.empty() ? text_path : bin_path;
+    if (access(in_path.c_str(), F_OK) == -1) {
+        fprintf(stderr, "File \"%s\" does not exist.\n", in_path.c_str());
+        return 1;
+    }
+    if (threshold <= 0.0f || threshold >= 1.0) {
+        fprintf(stderr, "Threshold must be a float in the range (0.0..1.0).\n");
+        return 1;
+    }
+    fprintf(stderr, "Document: %s\n", in_path.c_str());
+    fprintf(stderr, "Algorithm: %s\n", "fgssjoin");
+    fprintf(stderr, "Threshold: Jaccard %g\n", threshold);
+
+    fgss_options o;
+    fgss_options_default(&o);
+    o.device = device;
+    o.verbose = verbose;
+    fgss_ctx* ctx = nullptr;
+    fgss_status st = fgss_create(&ctx, &o);
+    if (st != FGSS_OK) return die(nullptr, st, "fgss_create");
+
+    fprintf(stderr, "... LOADING DATASET ...\n");
+    fgss_sets sets;
+    memset(&sets, 0, sizeof sets);
+    if (!bin_path.empty()) {
+        st = fgss_load_bin(bin_path.c_str(), &sets);
+        if (st != FGSS_OK) return die(ctx, st, "fgss_load_bin");
+    } else {
+        FILE* f = fopen(text_path.c_str(), "rb");
+        if (!f) return die(ctx, FGSS_ERR_IO, "open");
+        fseek(f, 0, SEEK_END);
+        long sz = ftell(f);
+        fseek(f, 0, SEEK_SET);
+        std::vector<char> buf((size_t)(sz > 0 ? sz : 0));
+        if (sz > 0 && fread(buf.data(), 1, (size_t)sz, f) != (size_t)sz) return die(ctx, FGSS_ERR_IO, "read");
+        fclose(f);
+        fgss_tok_opts to;
+        fgss_tok_opts_default(&to);
+        to.q = q;
+        to.mode = kmer ? FGSS_TOK_KMER : FGSS_TOK_QGRAM;
+        to.pad = pad;
+        to.suffix = suffix;
+        st = fgss_tokenize(ctx, buf.data(), buf.size(), &to, &sets);
+        if (st != FGSS_OK) return die(ctx, st, "fgss_tokenize");
+        if (!write_bin.empty()) {
+            std::string loc = write_bin + ".loc";
+            st = fgss_write_bin(write_bin.c_str(), loc.c_str(), &sets);
+            if (st != FGSS_OK) return die(ctx, st, "fgss_write_bin");
+        }
+    }
+    double avg = sets.n_sets ? (double)sets.n_tokens / (double)sets.n_sets : 0.0;
+    fprintf(stderr, "# Records: %llu\n", (unsigned long long)sets.n_sets);
+    fprintf(stderr, "# Terms: %u\n", sets.n_terms);
+    fprintf(stderr, "# Tokens: %llu\n", (unsigned long long)sets.n_tokens);
+    fprintf(stderr, "# Average size: %g\n", avg);
+    if (debug) {
+        for (uint64_t i = 0; i < sets.n_sets; i++) {
+            fprintf(stdout, "id: [%u]\nsize: [%u]\n", sets.id[i], sets.len[i]);
+            for (uint32_t j = 0; j < sets.len[i]; j++) fprintf(stdout, "(%u) ", sets.tokens[sets.pos[i] + j]);
+            fprintf(stdout, "\n\n");
+        }
+    }
+    fprintf(stderr, "=== BEGIN JOIN (TIMER STARTED) ===\n");
+    double t0 = now_us();
+    fgss_sets_view v = fgss_sets_view_of(&sets);
+    fgss_join_opts jo;
+    fgss_join_opts_default(&jo);
+    jo.threshold = threshold;
+    jo.method = method;
+    jo.bounds = bounds;
+    fgss_pairs pairs;
+    fgss_stats stats;
+    st = fgss_selfjoin(ctx, &v, &jo, &pairs, &stats);
+    if (st != FGSS_OK) return die(ctx, st, "fgss_selfjoin");
+    fprintf(stderr, "# Inverted Index Entries: %llu\n", (unsigned long long)stats.index_entries);
+    double r0 = now_us();
+    fgss_pairs_print(&pairs, stdout);
+    double r1 = now_us();
+    fprintf(stderr, "# Candidates: %llu\n", (unsigned long long)stats.candidates);
+    fprintf(stderr, "# Intersections: %llu\n", (unsigned long long)stats.intersections);
+    fprintf(stderr, "# Results: %llu\n", (unsigned long long)stats.results);
+    fprintf(stderr, "  - Time rendering: %g ms\n", (r1 - r0) / 1000.0);
+    double t1 = now_us();
+    fprintf(stderr, "===  END JOIN (TIMER STOPPED)  ===\n");
+    fprintf(stderr, "Total Running Time: %g s\n", (t1 - t0) / 1e6);
+    if (verbose)
+        fprintf(stderr, "# Device ms: index %.3f, filter+verify %.3f, output %.3f\n", stats.ms_index, stats.ms_filter,
+                stats.ms_output);
+    fgss_pairs_free(&pairs);
+    fgss_sets_free(&sets);
+    fgss_destroy(ctx);
+    return 0;
+}

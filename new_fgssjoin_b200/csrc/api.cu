@@ -1,0 +1,398 @@
+// api.cu -- the extern "C" boundary of libfgss (include/fgss.h).  Every entry
+// point catches the library's internal errors and returns a status; nothing
+// here exits the process (the reference calls exit(1) on any CUDA error,
+// src/util.cu:43-49).
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <memory>
+#include <vector>
+
+#include "join.h"
+#include "model.h"
+#include "prims.cuh"
+#include "tokenize.h"
+
+using namespace fgss;
+
+namespace {
+
+thread_local std::string g_err;
+
+template <typename F>
+fgss_status guard(fgss_ctx* ctx, F&& f) {
+    try {
+        f();
+        if (ctx) ctx->c.last_error.clear();
+        return FGSS_OK;
+    } catch (const Error& e) {
+        if (ctx) ctx->c.last_error = e.msg;
+        g_err = e.msg;
+        return e.st;
+    } catch (const std::bad_alloc&) {
+        if (ctx) ctx->c.last_error = "host allocation failed";
+        return FGSS_ERR_NOMEM;
+    } catch (...) {
+        if (ctx) ctx->c.last_error = "unknown error";
+        return FGSS_ERR_CUDA;
+    }
+}
+
+struct PairsPriv {
+    bool host_owned;
+};
+
+void fill_stats(const JoinState& J, fgss_stats* st) {
+    if (!st) return;
+    st->candidates = J.stats_host[SS_CANDIDATES];
+    st->intersections = J.stats_host[SS_INTERSECTIONS];
+    st->results = J.n_res;
+    st->probe_tokens = J.stats_host[SS_PROBE];
+    st->window_entries = J.stats_host[SS_WINDOW];
+    st->verified = J.stats_host[SS_VERIFIED];
+    st->heavy_queries = J.stats_host[SS_HEAVY];
+    st->overflow_retries = J.overflow_retries;
+    st->merged_tokens = J.stats_host[SS_MERGED];
+}
+
+void export_pairs(Ctx& c, JoinState& J, const fgss_join_opts& o, fgss_pairs* out) {
+    memset(out, 0, sizeof *out);
+    const uint64_t R = J.n_res;
+    out->n = R;
+    if (o.out_on_device) {
+        // hand out library buffers: copies so the context can be reused
+        auto dup = [&](const void* src, size_t bytes) -> void* {
+            void* p = nullptr;
+            FGSS_CK(cudaMalloc(&p, bytes ? bytes : 4));
+            if (bytes) FGSS_CK(cudaMemcpyAsync(p, src, bytes, cudaMemcpyDeviceToDevice, c.stream));
+            return p;
+        };
+        out->q = (uint32_t*)dup(J.oq, R * 4);
+        out->s = (uint32_t*)dup(J.os, R * 4);
+        out->id_q = (uint32_t*)dup(J.oidq, R * 4);
+        out->id_s = (uint32_t*)dup(J.oids, R * 4);
+        out->overlap = (uint32_t*)dup(J.oo, R * 4);
+        out->sim = (float*)dup(J.osim, R * 4);
+        out->on_device = 1;
+    } else {
+        const size_t b = (R ? R : 1) * 4;
+        out->q = (uint32_t*)malloc(b);
+        out->s = (uint32_t*)malloc(b);
+        out->id_q = (uint32_t*)malloc(b);
+        out->id_s = (uint32_t*)malloc(b);
+        out->overlap = (uint32_t*)malloc(b);
+        out->sim = (float*)malloc(b);
+        if (!out->q || !out->s || !out->id_q || !out->id_s || !out->overlap || !out->sim)
+            fail(FGSS_ERR_NOMEM, "host allocation for pairs");
+        if (R) {
+            FGSS_CK(cudaMemcpyAsync(out->q, J.oq, R * 4, cudaMemcpyDeviceToHost, c.stream));
+            FGSS_CK(cudaMemcpyAsync(out->s, J.os, R * 4, cudaMemcpyDeviceToHost, c.stream));
+            FGSS_CK(cudaMemcpyAsync(out->id_q, J.oidq, R * 4, cudaMemcpyDeviceToHost, c.stream));
+            FGSS_CK(cudaMemcpyAsync(out->id_s, J.oids, R * 4, cudaMemcpyDeviceToHost, c.stream));
+            FGSS_CK(cudaMemcpyAsync(out->overlap, J.oo, R * 4, cudaMemcpyDeviceToHost, c.stream));
+            FGSS_CK(cudaMemcpyAsync(out->sim, J.osim, R * 4, cudaMemcpyDeviceToHost, c.stream));
+        }
+        out->on_device = 0;
+    }
+    if (!J.cand_host.empty() || o.want_candidates) {
+        out->n_cand = J.cand_host.size() / 3;
+        out->cand = (uint32_t*)malloc((J.cand_host.size() + 1) * 4);
+        if (!J.cand_host.empty()) memcpy(out->cand, J.cand_host.data(), J.cand_host.size() * 4);
+    }
+    c.sync();
+}
+
+void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, int n, fgss_pairs* outs,
+               fgss_stats* stats) {
+    if (n <= 0) return;
+    if (!sets || !opts || !outs) fail(FGSS_ERR_INVALID, "null argument");
+    std::vector<std::unique_ptr<JoinState>> js(n);
+    cudaEvent_t* ev = c.ev;
+    const unsigned long long launches0 = launch_counter();
+    c.probe_timed = false;
+    FGSS_CK(cudaEventRecord(ev[0], c.stream));
+    for (int i = 0; i < n; i++) {
+        js[i].reset(new JoinState());
+        join_setup(c, *js[i], sets[i], opts[i], i);
+        join_index(c, *js[i]);
+    }
+    FGSS_CK(cudaEventRecord(ev[1], c.stream));
+    bool batched = false;
+    for (int i = 0; i < n; i++) batched |= opts[i].method == FGSS_METHOD_BATCHED;
+    if (batched) {
+        std::vector<JoinState*> v;
+        for (int i = 0; i < n; i++) v.push_back(js[i].get());
+        batched_filter_verify(c, v, opts[0].use_model != 0);
+        if (opts[0].want_candidates) fail(FGSS_ERR_INVALID, "want_candidates needs the plain method");
+    } else {
+        for (int i = 0; i < n; i++) join_plain_filter_verify(c, *js[i], opts[i].want_candidates != 0);
+    }
+    FGSS_CK(cudaEventRecord(ev[2], c.stream));
+    for (int i = 0; i < n; i++) {
+        join_finish_status(c, *js[i]);
+        export_pairs(c, *js[i], opts[i], &outs[i]);
+    }
+    FGSS_CK(cudaEventRecord(ev[3], c.stream));
+    FGSS_CK(cudaEventSynchronize(ev[3]));
+    float t_idx = 0, t_fv = 0, t_out = 0;
+    FGSS_CK(cudaEventElapsedTime(&t_idx, ev[0], ev[1]));
+    FGSS_CK(cudaEventElapsedTime(&t_fv, ev[1], ev[2]));
+    FGSS_CK(cudaEventElapsedTime(&t_out, ev[2], ev[3]));
+    float t_probe = 0;
+    if (c.probe_timed) FGSS_CK(cudaEventElapsedTime(&t_probe, ev[4], ev[5]));
+    const unsigned long long launches = launch_counter() - launches0;
+    if (stats) {
+        for (int i = 0; i < n; i++) {
+            memset(&stats[i], 0, sizeof(fgss_stats));
+            fill_stats(*js[i], &stats[i]);
+            stats[i].index_entries = 0;
+            stats[i].ms_index = t_idx;
+            stats[i].ms_filter = t_fv;
+            stats[i].ms_output = t_out;
+            stats[i].ms_total = t_idx + t_fv + t_out;
+            stats[i].ms_probe = t_probe;
+            stats[i].launches = launches;
+        }
+        // index entries: device count
+        for (int i = 0; i < n; i++) {
+            uint64_t e = 0;
+            FGSS_CK(cudaMemcpy(&e, js[i]->d_e, 8, cudaMemcpyDeviceToHost));
+            stats[i].index_entries = e;
+        }
+    }
+    if (c.verbose)
+        fprintf(stderr, "[fgss] joins=%d index %.3f ms, filter+verify %.3f ms, output %.3f ms\n", n, t_idx, t_fv,
+                t_out);
+}
+
+}  // namespace
+
+extern "C" {
+
+int fgss_version(void) { return FGSS_VERSION_MAJOR * 100 + FGSS_VERSION_MINOR; }
+
+const char* fgss_strerror(fgss_status st) {
+    switch (st) {
+        case FGSS_OK: return "ok";
+        case FGSS_ERR_INVALID: return "invalid argument";
+        case FGSS_ERR_CUDA: return "CUDA error";
+        case FGSS_ERR_NOMEM: return "out of memory";
+        case FGSS_ERR_FORMAT: return "malformed input";
+        case FGSS_ERR_IO: return "I/O error";
+        case FGSS_ERR_UNSUPPORTED: return "unsupported input";
+        case FGSS_ERR_TIMEOUT: return "device wait timed out";
+        case FGSS_ERR_CAPACITY: return "buffer too small";
+    }
+    return "unknown status";
+}
+
+const char* fgss_last_error(const fgss_ctx* ctx) { return ctx ? ctx->c.last_error.c_str() : g_err.c_str(); }
+
+void fgss_options_default(fgss_options* o) {
+    if (!o) return;
+    memset(o, 0, sizeof *o);
+}
+
+void fgss_join_opts_default(fgss_join_opts* o) {
+    if (!o) return;
+    memset(o, 0, sizeof *o);
+    o->threshold = 0.9f;
+    o->bounds = FGSS_BOUNDS_REFERENCE;
+    o->method = FGSS_METHOD_PLAIN;
+}
+
+void fgss_tok_opts_default(fgss_tok_opts* o) {
+    if (!o) return;
+    o->q = 3;
+    o->mode = FGSS_TOK_QGRAM;
+    o->pad = 0;
+    o->pad_char = 1;
+    o->suffix = 1;
+    o->lower = 1;
+}
+
+fgss_status fgss_create(fgss_ctx** out, const fgss_options* opt) {
+    if (!out) return FGSS_ERR_INVALID;
+    *out = nullptr;
+    fgss_ctx* ctx = new (std::nothrow) fgss_ctx();
+    if (!ctx) return FGSS_ERR_NOMEM;
+    fgss_status st = guard(ctx, [&] {
+        fgss_options o;
+        fgss_options_default(&o);
+        if (opt) o = *opt;
+        Ctx& c = ctx->c;
+        int ndev = 0;
+        FGSS_CK(cudaGetDeviceCount(&ndev));
+        if (o.device < 0 || o.device >= ndev) fail(FGSS_ERR_INVALID, "no such CUDA device");
+        c.device = o.device;
+        FGSS_CK(cudaSetDevice(c.device));
+        cudaDeviceProp prop;
+        FGSS_CK(cudaGetDeviceProperties(&prop, c.device));
+        if (prop.major != 10) fail(FGSS_ERR_UNSUPPORTED, "libfgss is built for sm_100a (B200) only");
+        c.num_sms = prop.multiProcessorCount;
+        c.smem_optin = prop.sharedMemPerBlockOptin;
+        c.verbose = o.verbose;
+        if (o.tune_cache_path) c.tune_path = o.tune_cache_path;
+        if (o.stream) {
+            c.stream = (cudaStream_t)o.stream;
+            c.own_stream = false;
+        } else {
+            FGSS_CK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+            c.own_stream = true;
+        }
+        for (auto& e : c.ev) FGSS_CK(cudaEventCreate(&e));
+    });
+    if (st != FGSS_OK) {
+        g_err = ctx->c.last_error;
+        delete ctx;
+        return st;
+    }
+    *out = ctx;
+    return FGSS_OK;
+}
+
+void fgss_destroy(fgss_ctx* ctx) {
+    if (!ctx) return;
+    Ctx& c = ctx->c;
+    cudaSetDevice(c.device);
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    for (auto& kv : c.bufs)
+        if (kv.second.p) cudaFree(kv.second.p);
+    for (auto& kv : c.host_bufs)
+        if (kv.second.p) cudaFreeHost(kv.second.p);
+    for (auto& e : c.ev)
+        if (e) cudaEventDestroy(e);
+    if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
+    delete c.model;
+    delete ctx;
+}
+
+fgss_sets_view fgss_sets_view_of(const fgss_sets* s) {
+    fgss_sets_view v;
+    memset(&v, 0, sizeof v);
+    if (!s) return v;
+    v.id = s->id;
+    v.pos = s->pos;
+    v.len = s->len;
+    v.tokens = s->tokens;
+    v.n_sets = s->n_sets;
+    v.n_tokens = s->n_tokens;
+    v.n_terms = s->n_terms;
+    v.on_device = 0;
+    return v;
+}
+
+void fgss_sets_free(fgss_sets* s) {
+    if (!s) return;
+    free(s->id);
+    free(s->pos);
+    free(s->len);
+    free(s->tokens);
+    free(s->loc);
+    memset(s, 0, sizeof *s);
+}
+
+fgss_status fgss_tokenize(fgss_ctx* ctx, const char* text, uint64_t n_bytes, const fgss_tok_opts* opts,
+                          fgss_sets* out) {
+    if (!ctx || !out || (!text && n_bytes)) return FGSS_ERR_INVALID;
+    return guard(ctx, [&] {
+        fgss_tok_opts o;
+        fgss_tok_opts_default(&o);
+        if (opts) o = *opts;
+        TokParams p{o.q, o.mode, o.pad, o.pad_char, o.suffix, o.lower};
+        FGSS_CK(cudaSetDevice(ctx->c.device));
+        try {
+            tokenize_device(ctx->c, text, n_bytes, p, out);
+        } catch (...) {
+            fgss_sets_free(out);
+            throw;
+        }
+    });
+}
+
+fgss_status fgss_selfjoin(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_join_opts* opts, fgss_pairs* out,
+                          fgss_stats* stats) {
+    if (!ctx || !sets || !opts || !out) return FGSS_ERR_INVALID;
+    return guard(ctx, [&] {
+        FGSS_CK(cudaSetDevice(ctx->c.device));
+        run_joins(ctx->c, sets, opts, 1, out, stats);
+    });
+}
+
+fgss_status fgss_selfjoin_batch(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_join_opts* opts, int n,
+                                fgss_pairs* outs, fgss_stats* stats) {
+    if (!ctx || !sets || !opts || !outs || n < 0) return FGSS_ERR_INVALID;
+    return guard(ctx, [&] {
+        FGSS_CK(cudaSetDevice(ctx->c.device));
+        run_joins(ctx->c, sets, opts, n, outs, stats);
+    });
+}
+
+void fgss_pairs_free(fgss_pairs* p) {
+    if (!p) return;
+    if (p->on_device) {
+        cudaFree(p->q);
+        cudaFree(p->s);
+        cudaFree(p->id_q);
+        cudaFree(p->id_s);
+        cudaFree(p->overlap);
+        cudaFree(p->sim);
+    } else {
+        free(p->q);
+        free(p->s);
+        free(p->id_q);
+        free(p->id_s);
+        free(p->overlap);
+        free(p->sim);
+    }
+    free(p->cand);
+    memset(p, 0, sizeof *p);
+}
+
+fgss_status fgss_pairs_print(const fgss_pairs* p, void* file) {
+    if (!p) return FGSS_ERR_INVALID;
+    if (p->on_device) return FGSS_ERR_INVALID;
+    FILE* f = file ? (FILE*)file : stdout;
+    for (uint64_t i = 0; i < p->n; i++)
+        fprintf(f, "%d %d %f\n", (int)p->id_q[i], (int)p->id_s[i], (double)p->sim[i]);  // block.cu:193
+    return FGSS_OK;
+}
+
+fgss_status fgss_bounds_table(float threshold, int bounds, uint32_t max_len, uint16_t* probe, uint16_t* index,
+                              uint32_t* min_size, uint32_t* max_size, uint32_t* need) {
+    if (max_len > kMaxLen) return FGSS_ERR_UNSUPPORTED;
+    if (!(threshold > 0.0f && threshold < 1.0f) || (bounds != 0 && bounds != 1)) return FGSS_ERR_INVALID;
+    BoundTables b;
+    compute_bounds(threshold, bounds, b);
+    for (uint32_t n = 0; n <= max_len; n++) {
+        if (probe) probe[n] = b.probe[n];
+        if (index) index[n] = b.index[n];
+        if (min_size) min_size[n] = b.minsz[n];
+        if (max_size) max_size[n] = b.maxsz[n];
+    }
+    if (need)
+        for (uint32_t S = 0; S <= 2 * max_len; S++) need[S] = b.need[S];
+    return FGSS_OK;
+}
+
+fgss_status fgss_dev_exclusive_scan_u32(fgss_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t n) {
+    if (!ctx || (n && (!in || !out))) return FGSS_ERR_INVALID;
+    return guard(ctx, [&] {
+        FGSS_CK(cudaSetDevice(ctx->c.device));
+        if (n) exclusive_scan<uint32_t>(ctx->c, in, out, n, nullptr, (uint32_t*)nullptr, "api.scan");
+        ctx->c.sync();
+    });
+}
+
+fgss_status fgss_dev_sort_pairs_u64(fgss_ctx* ctx, uint64_t* keys, uint32_t* values, uint64_t n, int begin_bit,
+                                    int end_bit) {
+    if (!ctx || (n && !keys) || begin_bit < 0 || end_bit > 64 || begin_bit > end_bit) return FGSS_ERR_INVALID;
+    return guard(ctx, [&] {
+        FGSS_CK(cudaSetDevice(ctx->c.device));
+        if (n) radix_sort<uint64_t, uint32_t>(ctx->c, keys, values, n, nullptr, begin_bit, end_bit, "api.sort");
+        ctx->c.sync();
+    });
+}
+
+}  // extern "C"

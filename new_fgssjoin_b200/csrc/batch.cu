@@ -1,0 +1,263 @@
+// batch.cu -- the batched method: per-query features and cost, balanced work
+// items, one persistent fused filter+verify launch over every join of a
+// batch, presized result buffers with an exact re-run on overflow.
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "join.h"
+#include "model.h"
+#include "prims.cuh"
+
+namespace fgss {
+
+// Per query: features of the cost model and the heuristic cost
+// (sum of the probe tokens' full list lengths, plus the query size).
+__global__ void k_features(JoinArgs a, float t, float* __restrict__ feat, uint32_t* __restrict__ cost) {
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t lane = lane_id();
+    for (uint32_t q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < a.n; q += warps) {
+        uint32_t lq = a.len[q];
+        uint32_t qp = lq <= 65535u ? a.probe[lq] : 0;
+        const uint32_t* qt = a.tok + a.pos[q];
+        unsigned long long sum = 0;
+        uint32_t mx = 0;
+        float slog = 0.f;
+        for (uint32_t j = lane; j < qp; j += 32) {
+            uint32_t w = __ldg(qt + j);
+            uint32_t l = __ldg(a.list_off + w + 1) - __ldg(a.list_off + w);
+            sum += l;
+            mx = max(mx, l);
+            slog += log1pf((float)l);
+        }
+        sum = warp_sum(sum);
+        mx = __reduce_max_sync(kFull, mx);
+        slog = warp_sum(slog);
+        if (lane == 0) {
+            uint32_t send = lq <= 65535u ? a.send[lq] : q + 1;
+            uint32_t win = send > q + 1 ? send - q - 1 : 0;
+            float* f = feat + (uint64_t)q * kFeat;
+            f[0] = log1pf((float)lq);
+            f[1] = log1pf((float)qp);
+            f[2] = log1pf((float)sum);
+            f[3] = log1pf((float)mx);
+            f[4] = qp ? slog / (float)qp : 0.f;
+            f[5] = log1pf((float)win);
+            f[6] = a.n ? (float)q / (float)a.n : 0.f;
+            f[7] = t;
+            unsigned long long c = sum + lq;
+            cost[q] = (uint32_t)min(c, 0x3fffffffull);
+        }
+    }
+}
+
+// Work items of one join: item k = queries with exclusive cost prefix in
+// [k*target, (k+1)*target).
+__global__ void k_items(const uint32_t* __restrict__ pre, uint32_t n, uint64_t total, uint32_t K, uint32_t join,
+                        uint4* __restrict__ items) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+        uint64_t target = (total + K - 1) / K;
+        auto first_ge = [&](uint64_t x) {
+            uint32_t lo = 0, hi = n;
+            while (lo < hi) {
+                uint32_t mid = (lo + hi) >> 1;
+                if ((uint64_t)pre[mid] < x) lo = mid + 1;
+                else hi = mid;
+            }
+            return lo;
+        };
+        uint32_t b = k == 0 ? 0 : first_ge(k * target);
+        uint32_t e = k + 1 == K ? n : first_ge((k + 1) * target);
+        items[k] = make_uint4(join, b, max(b, e), 0);
+    }
+}
+
+template <int NT, int HLOG>
+static void launch_fused(Ctx& c, const JoinArgs* d_args, const uint4* items, uint32_t n_items, uint32_t* counter,
+                         int ctas_per_sm) {
+    static bool attr = false;
+    const size_t smem = ProbeLayout<MODE_FUSED, HLOG>::bytes;
+    if (!attr) {
+        FGSS_CK(cudaFuncSetAttribute(k_probe<MODE_FUSED, NT, HLOG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+        attr = true;
+    }
+    int occ = 0;
+    FGSS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_probe<MODE_FUSED, NT, HLOG>, NT, smem));
+    if (occ < 1) occ = 1;
+    int per = std::min(occ, std::max(1, ctas_per_sm));
+    unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)per * c.num_sms, std::max<uint32_t>(n_items, 1));
+    k_probe<MODE_FUSED, NT, HLOG><<<grid, NT, smem, c.stream>>>(d_args, items, n_items, counter);
+    FGSS_LAUNCH_CK();
+}
+
+void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const uint4* items, uint32_t n_items,
+                  uint32_t* counter) {
+#define FGSS_F(NT, HL)                                                            \
+    if (te.threads == NT && te.hash_log2 == HL) {                                 \
+        launch_fused<NT, HL>(c, d_args, items, n_items, counter, te.ctas_per_sm); \
+        return;                                                                   \
+    }
+    FGSS_F(256, 12)
+    FGSS_F(256, 13)
+    FGSS_F(512, 12)
+    FGSS_F(512, 13)
+    FGSS_F(512, 14)
+#undef FGSS_F
+    launch_fused<256, 12>(c, d_args, items, n_items, counter, te.ctas_per_sm);
+}
+
+// Resets the filter's counters and overflow bit of one join before a re-run
+// (the input-validation bits and the probe-token count stay).
+__global__ void k_clear_filter_state(uint32_t* status, unsigned long long* stats) {
+    if (threadIdx.x == 0) {
+        status[0] &= ~(uint32_t)(ST_RES_OVERFLOW | ST_HEAVY_OVERFLOW | ST_HASH_FULL);
+        status[2] = 0;
+        status[3] = 0;
+    }
+    if (threadIdx.x < SS_N && threadIdx.x != SS_PROBE) stats[threadIdx.x] = 0;
+}
+
+// Runs the fused filter+verify over every join (their index built already).
+void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_model) {
+    const size_t nj = joins.size();
+    uint64_t* d_tot = c.devT<uint64_t>("b.tot", nj * 2 + 2);
+    std::vector<uint32_t*> pre(nj);
+    FGSS_CK(cudaMemsetAsync(d_tot, 0, (nj * 2 + 2) * 8, c.stream));
+    for (size_t i = 0; i < nj; i++) {
+        JoinState& J = *joins[i];
+        const uint64_t n = J.in.n_sets;
+        float* feat = c.devT<float>(J.pfx("feat"), (n + 1) * kFeat);
+        uint32_t* cost = c.devT<uint32_t>(J.pfx("cost"), n + 1);
+        pre[i] = c.devT<uint32_t>(J.pfx("cpre"), n + 1);
+        if (n == 0) continue;
+        k_features<<<grid_for(n * 32, 256, c.num_sms * 32), 256, 0, c.stream>>>(J.args, J.t, feat, cost);
+        FGSS_LAUNCH_CK();
+        if (use_model && c.model) model_predict(c, feat, n, cost, &d_tot[nj + i]);
+        exclusive_scan<uint32_t>(c, cost, pre[i], n, nullptr, (uint32_t*)nullptr, J.pfx("scan.cost").c_str());
+        // total cost (64-bit)
+        model_sum_cost(c, cost, n, &d_tot[i]);
+    }
+    std::vector<uint64_t> htot(2 * nj + 2);
+    FGSS_CK(cudaMemcpyAsync(htot.data(), d_tot, (2 * nj + 2) * 8, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    uint64_t grand = 0;
+    for (size_t i = 0; i < nj; i++) grand += htot[i];
+    // items: ~16 per resident CTA over the whole batch, split by cost share
+    const TuneEntry te = c.tune.count("fused") ? c.tune["fused"] : TuneEntry{};
+    const uint64_t want = (uint64_t)16 * c.num_sms * std::max(1, te.ctas_per_sm);
+    std::vector<uint32_t> K(nj, 0);
+    uint64_t nitems = 0;
+    for (size_t i = 0; i < nj; i++) {
+        const uint64_t n = joins[i]->in.n_sets;
+        if (n == 0) continue;
+        uint64_t k = grand ? (want * htot[i] + grand - 1) / grand : 1;
+        k = std::max<uint64_t>(1, std::min<uint64_t>(k, n));
+        K[i] = (uint32_t)k;
+        nitems += k;
+    }
+    uint4* items = c.devT<uint4>("b.items", nitems + 1);
+    uint64_t off = 0;
+    for (size_t i = 0; i < nj; i++) {
+        if (!K[i]) continue;
+        JoinState& J = *joins[i];
+        if (htot[i] >= (1ull << 32)) fail(FGSS_ERR_UNSUPPORTED, "cost prefix exceeds 32 bits");
+        k_items<<<grid_for(K[i], 128), 128, 0, c.stream>>>(pre[i], (uint32_t)J.in.n_sets, htot[i], K[i],
+                                                            (uint32_t)i, items + off);
+        FGSS_LAUNCH_CK();
+        off += K[i];
+    }
+    // result buffers: the learned estimate (x1.5 + slack) or the last size seen
+    JoinArgs* d_args = c.devT<JoinArgs>("b.args", nj);
+    std::vector<JoinArgs> hargs(nj);
+    for (size_t i = 0; i < nj; i++) {
+        JoinState& J = *joins[i];
+        const uint64_t n = J.in.n_sets;
+        uint64_t cap;
+        auto itc = c.tune.find(J.pfx("rescap"));
+        const uint64_t last = itc != c.tune.end() ? (uint64_t)itc->second.ctas_per_sm : 0;
+        if (J.res_cap_hint) {
+            cap = J.res_cap_hint;
+        } else if (use_model && c.model) {
+            cap = (uint64_t)((double)htot[nj + i] * 1.5) + 4096;  // predicted results x 1.5 + slack
+        } else {
+            cap = std::max<uint64_t>(n + 4096, last);
+        }
+        cap = std::min<uint64_t>(cap, 0xfffffff0ull);
+        JoinArgs& a = J.args;
+        a.res_cap = (uint32_t)cap;
+        a.res_q = c.devT<uint32_t>(J.pfx("res.q"), cap + 1);
+        a.res_s = c.devT<uint32_t>(J.pfx("res.s"), cap + 1);
+        a.res_o = c.devT<uint32_t>(J.pfx("res.o"), cap + 1);
+        a.res_count = J.status + 3;
+        FGSS_CK(cudaMemsetAsync(a.heavy_count, 0, 8, c.stream));  // heavy_count + res_count
+        hargs[i] = a;
+    }
+    FGSS_CK(cudaMemcpyAsync(d_args, hargs.data(), nj * sizeof(JoinArgs), cudaMemcpyHostToDevice, c.stream));
+    uint32_t* counter = c.devT<uint32_t>("b.counter", 4 + nj);
+    FGSS_CK(cudaMemsetAsync(counter, 0, (4 + nj) * 4, c.stream));
+    FGSS_CK(cudaEventRecord(c.ev[4], c.stream));
+    if (nitems) fused_launch(c, te, d_args, items, (uint32_t)nitems, counter);
+    FGSS_CK(cudaEventRecord(c.ev[5], c.stream));
+    c.probe_timed = true;
+    // heavy queries: read the queue sizes, one persistent launch per join
+    std::vector<uint32_t> hq(2 * nj);
+    uint32_t* hbuf = c.pinnedT<uint32_t>("b.hq", 2 * nj + 2);
+    for (size_t i = 0; i < nj; i++)
+        FGSS_CK(cudaMemcpyAsync(hbuf + 2 * i, joins[i]->status + 2, 8, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    for (size_t i = 0; i < nj; i++) {
+        uint32_t nh = hbuf[2 * i];
+        if (!nh) continue;
+        JoinState& J = *joins[i];
+        uint32_t slots = std::min<uint32_t>(nh, (uint32_t)c.num_sms);
+        uint64_t words = 4 * J.in.n_sets + 65536 + 65537;
+        words = (words + 63) & ~63ull;
+        const std::string name = "heavy.scratch";
+        auto it = c.bufs.find(name);
+        size_t need = words * slots * 4;
+        bool grow = it == c.bufs.end() || it->second.bytes < need;
+        uint32_t* scratch = (uint32_t*)c.dev(name, need);
+        if (grow) FGSS_CK(cudaMemsetAsync(scratch, 0, c.bufs[name].bytes, c.stream));
+        k_probe_heavy<MODE_FUSED, 512><<<slots, 512, 0, c.stream>>>(d_args, (uint32_t)i, scratch, words,
+                                                                    counter + 4 + i);
+        FGSS_LAUNCH_CK();
+    }
+    // results: overflow -> exact re-run of that join with the exact capacity
+    for (size_t i = 0; i < nj; i++)
+        FGSS_CK(cudaMemcpyAsync(hbuf + 2 * i, joins[i]->status + 3, 4, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    for (size_t i = 0; i < nj; i++) {
+        JoinState& J = *joins[i];
+        const uint32_t got = hbuf[2 * i];
+        if (got > J.args.res_cap) {
+            // The learned (or remembered) capacity was too small: the kernel kept
+            // counting, so re-run this join alone with the exact size.
+            J.res_cap_hint = got;
+            J.overflow_retries++;
+            k_clear_filter_state<<<1, 32, 0, c.stream>>>(J.status, J.stats);
+            FGSS_LAUNCH_CK();
+            std::vector<JoinState*> one{&J};
+            batched_filter_verify(c, one, false);
+            continue;
+        }
+        // remember a sufficient capacity for the next call on this slot
+        J.res_cap_hint = 0;
+        c.tune[J.pfx("rescap")].ctas_per_sm = (int)std::min<uint64_t>((uint64_t)got + got / 4 + 1024, 0x7fffffff);
+        uint64_t* keys = c.devT<uint64_t>(J.pfx("rkey"), (uint64_t)J.args.res_cap + 1);
+        uint32_t* vals = c.devT<uint32_t>(J.pfx("rval"), (uint64_t)J.args.res_cap + 1);
+        J.d_nres = c.devT<uint64_t>(J.pfx("nres"), 2);
+        if (got) {
+            k_result_keys<<<grid_for(got, 256, c.num_sms * 32), 256, 0, c.stream>>>(
+                J.args.res_q, J.args.res_s, J.args.res_o, J.status + 3, J.args.res_cap, keys, vals, J.d_nres);
+            FGSS_LAUNCH_CK();
+        } else {
+            FGSS_CK(cudaMemsetAsync(J.d_nres, 0, 8, c.stream));
+        }
+        join_output(c, J, keys, vals, J.d_nres, got);
+        J.n_res = got;
+    }
+}
+
+}  // namespace fgss

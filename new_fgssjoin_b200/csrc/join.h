@@ -1,0 +1,73 @@
+// join.h -- host driver of the self-join (plain and batched methods).
+#pragma once
+
+#include <vector>
+
+#include "bounds.h"
+#include "ctx.h"
+#include "join_kernels.cuh"
+
+namespace fgss {
+
+// Device tables of one threshold (cached in the context per (t, mode)).
+struct DevBounds {
+    uint16_t* probe;
+    uint16_t* index;
+    uint32_t* minsz;
+    uint32_t* maxsz;
+    uint32_t* lmin;
+    uint32_t* cand_min;
+    uint32_t* inter_min;
+    uint32_t* need;
+};
+DevBounds device_bounds(Ctx& c, float t, int mode);
+
+// Per-query features of the learned cost model (one row per record).
+constexpr int kFeat = 8;
+
+// Everything one join keeps on the device between stages.
+struct JoinState {
+    int slot = 0;              // buffer-name prefix (joins of a batch use different slots)
+    fgss_sets_view in{};       // device view
+    const uint32_t* id = nullptr;
+    float t = 0.f;
+    int bounds = 0;
+    DevBounds lut{};
+    JoinArgs args{};
+    JoinArgs* d_args = nullptr;
+    uint32_t* status = nullptr;
+    unsigned long long* stats = nullptr;
+    uint64_t* d_e = nullptr;   // index entries (u64 copy of the scan total)
+    uint32_t* icnt = nullptr;
+    uint32_t* pcnt = nullptr;
+    uint32_t* maxlen = nullptr;
+    int term_bits = 1;
+    // outputs (device)
+    uint64_t* d_nres = nullptr;
+    uint32_t *oq = nullptr, *os = nullptr, *oidq = nullptr, *oids = nullptr, *oo = nullptr;
+    float* osim = nullptr;
+    uint64_t n_res = 0;
+    uint64_t res_cap_hint = 0;   // exact result count after an overflow
+    uint32_t overflow_retries = 0;
+    uint32_t status_host = 0;
+    unsigned long long stats_host[SS_N] = {};
+    std::vector<uint32_t> cand_host;  // (q, s, partial) triples when requested
+    std::string pfx(const char* name) const { return "j" + std::to_string(slot) + "." + name; }
+};
+
+// Stage drivers (join.cu)
+void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_opts& o, int slot);
+void join_index(Ctx& c, JoinState& J);
+void join_plain_filter_verify(Ctx& c, JoinState& J, bool want_cand);
+void join_features(Ctx& c, JoinState& J, float* d_feat);
+void join_finish_status(Ctx& c, JoinState& J);  // D2H of status + stats, throws on bad input
+void join_output(Ctx& c, JoinState& J, uint64_t* keys, uint32_t* vals, const uint64_t* d_n, uint64_t n_cap);
+
+// Fused persistent filter+verify over many joins at once (batch.cu)
+struct BatchPlan {
+    std::vector<uint32_t> res_cap;   // per join
+    bool use_model = false;
+};
+void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_model);
+
+}  // namespace fgss

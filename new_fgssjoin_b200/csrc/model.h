@@ -1,0 +1,45 @@
+// model.h -- the learned cost model of the batched method: a 2-layer FP32 MLP
+// (kFeat inputs -> kHidden ReLU -> 2 outputs) predicting, per query record,
+// log1p(window entries the filter reads) and log1p(result pairs it emits).
+// Training and inference are our own CUDA kernels (model.cu).  The model is
+// advisory only: it sizes the result buffers and balances work items; an
+// undersized buffer is detected on the device and the join re-runs exactly.
+#pragma once
+
+#include <stdint.h>
+
+#include <vector>
+
+#include "ctx.h"
+
+namespace fgss {
+
+constexpr int kHidden = 32;
+constexpr int kOut = 2;
+constexpr int kFeatM = 8;  // equals kFeat in join.h
+// parameter block: W1[H][F] b1[H] W2[O][H] b2[O] calib[O]
+constexpr int kParams = kHidden * kFeatM + kHidden + kOut * kHidden + kOut;
+constexpr int kParamsAll = kParams + kOut;
+
+}  // namespace fgss
+
+struct fgss_model {
+    std::vector<float> host;   // kParamsAll floats
+    float* dev = nullptr;      // device copy
+    float last_loss = 0.f;
+    int trained = 0;
+};
+
+namespace fgss {
+
+// cost[q] <- expm1(pred window) + len (u32); *res_sum += sum of predicted results (x calib)
+void model_predict(Ctx& c, const float* feat, uint64_t n, uint32_t* cost, uint64_t* res_sum);
+// *out += sum of cost[0..n)
+void model_sum_cost(Ctx& c, const uint32_t* cost, uint64_t n, uint64_t* out);
+// Full-batch Adam training on (feat, target) rows already on the device;
+// target rows are (log1p window, log1p results).  Returns the final loss.
+float model_fit(Ctx& c, const float* feat, const float* target, uint64_t n, int epochs, float lr, uint64_t seed);
+// One gradient evaluation (for tests): params (kParams) -> grads (kParams), returns loss.
+float model_grad(Ctx& c, const float* feat, const float* target, uint64_t n, const float* params, float* grads);
+
+}  // namespace fgss

@@ -1,0 +1,201 @@
+"""GPU parity: the CUDA join through the C ABI against the CPU oracle."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+import new_fgssjoin_b200 as F
+from new_fgssjoin_b200 import datagen
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+THRESHOLDS = [0.5, 0.6, 0.7, 0.8, 0.9, 0.95]
+
+
+def _check_same(got, ref, st=None):
+    assert len(got) == len(ref)
+    assert np.array_equal(got.q, ref["q"])
+    assert np.array_equal(got.s, ref["s"])
+    assert np.array_equal(got.overlap, ref["overlap"])
+    assert np.array_equal(got.sim, ref["sim"])  # float32 division, bit-exact
+    if st is not None:
+        for k in ("candidates", "intersections", "results"):
+            assert got.stats[k] == st[k], (k, got.stats, st)
+        assert got.stats["index_entries"] == st["index_entries"]
+
+
+@pytest.mark.parametrize("method", ["plain", "batched"])
+@pytest.mark.parametrize("t", ["0.5", "0.59", "0.6", "0.7", "0.75", "0.8", "0.9"])
+def test_golden_fixture_pairs(ctx, method, t):
+    s = F.ppjoin_format(os.path.join(GOLDEN, "small.txt.3gram.bin"))
+    got = ctx.selfjoin(s, float(t), method=method)
+    gold = json.load(open(os.path.join(GOLDEN, "small_pairs.json")))[t]
+    assert sorted(got.lines()) == gold
+
+
+def _titles(n, seed):
+    return datagen.titles(n, seed=seed)
+
+
+@pytest.fixture(scope="module")
+def titles_sets(ctx):
+    return ctx.tokenize(_titles(6000, 11), **datagen.TITLE_TOK)
+
+
+@pytest.mark.parametrize("method", ["plain", "batched"])
+@pytest.mark.parametrize("t", THRESHOLDS)
+def test_titles_vs_oracle(ctx, titles_sets, method, t):
+    s = titles_sets
+    got = ctx.selfjoin(s, t, method=method)
+    ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, t)
+    _check_same(got, ref, st)
+
+
+@pytest.mark.parametrize("t", [0.5, 0.6, 0.8])
+def test_candidates_match_oracle(ctx, titles_sets, t):
+    """The plain method's candidate list (q, s, partial score) equals the reference filter's cells > 0,
+    restricted to the candidates a merge can still bring to floor(min overlap)."""
+    s = titles_sets
+    got = ctx.selfjoin(s, t, method="plain", want_candidates=True)
+    ref, st, cands = O.join(s.pos, s.len, s.tokens, s.n_terms, t, want_candidates=True)
+    assert got.stats["candidates"] == st["candidates"] == len(cands)
+    gc = {(int(a), int(b)): int(c) for a, b, c in got.candidates}
+    rc = {(int(a), int(b)): int(c) for a, b, c in cands}
+    assert set(gc) <= set(rc)
+    for k, v in gc.items():
+        assert rc[k] == v  # same partial score
+    # every pair the reference verifies to an intersection is among ours
+    verified = set(zip(ref["q"].tolist(), ref["s"].tolist()))
+    assert verified <= set(gc)
+
+
+def _random_sets(rng, n, vocab, lo, hi, sort=True):
+    lens = rng.integers(lo, hi + 1, n)
+    if sort:
+        lens = np.sort(lens)[::-1]
+    toks = [np.sort(rng.choice(vocab, size=int(l), replace=False)) for l in lens]
+    pos = np.zeros(n, np.uint32)
+    if n > 1:
+        pos[1:] = np.cumsum(lens[:-1])
+    tok = np.concatenate(toks).astype(np.uint32) if n else np.zeros(0, np.uint32)
+    return F.Sets(np.arange(1, n + 1), pos, lens, tok, vocab)
+
+
+@pytest.mark.parametrize("seed", range(4))
+@pytest.mark.parametrize("t", THRESHOLDS)
+def test_random_small_vocab(ctx, seed, t):
+    """Dense overlaps, equal sizes, lengths n = 0 (mod 9) and 0.6 n integral (float32 bound edges)."""
+    rng = np.random.default_rng(seed * 131 + int(t * 1000))
+    s = _random_sets(rng, 700, 60, 1, 45)
+    for method in ("plain", "batched"):
+        got = ctx.selfjoin(s, t, method=method)
+        ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, t)
+        _check_same(got, ref, st)
+
+
+@pytest.mark.parametrize("t", [0.6, 0.8])
+def test_unsorted_input_matches_reference_semantics(ctx, t):
+    """Records not in descending size: per-entry size filter and the one-tile skip test."""
+    rng = np.random.default_rng(5)
+    s = _random_sets(rng, 400, 50, 1, 30, sort=False)
+    for method in ("plain", "batched"):
+        got = ctx.selfjoin(s, t, method=method)
+        ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, t)
+        _check_same(got, ref, st)
+
+
+def test_empty_and_singleton_inputs(ctx):
+    empty = F.Sets(np.zeros(0), np.zeros(0), np.zeros(0), np.zeros(0), 0)
+    one = F.Sets([7], [0], [3], [1, 2, 3], 4)
+    for method in ("plain", "batched"):
+        assert len(ctx.selfjoin(empty, 0.5, method=method)) == 0
+        assert len(ctx.selfjoin(one, 0.5, method=method)) == 0
+
+
+def test_empty_records_take_part_in_no_pair(ctx):
+    s = F.Sets([1, 2, 3, 4], [0, 3, 6, 6], [3, 3, 0, 0], [1, 2, 3, 1, 2, 3], 4)
+    got = ctx.selfjoin(s, 0.5)
+    assert got.lines() == ["1 2 1.000000"]
+
+
+def test_identical_records(ctx):
+    n = 50
+    tok = np.tile(np.arange(10, dtype=np.uint32), n)
+    s = F.Sets(np.arange(1, n + 1), np.arange(n) * 10, np.full(n, 10), tok, 10)
+    got = ctx.selfjoin(s, 0.9, method="batched")
+    assert len(got) == n * (n - 1) // 2
+    assert np.all(got.overlap == 10) and np.all(got.sim == 1.0)
+
+
+def test_unsorted_tokens_rejected(ctx):
+    s = F.Sets([1, 2], [0, 3], [3, 3], [3, 2, 1, 1, 2, 3], 4)
+    with pytest.raises(F.FgssError) as e:
+        ctx.selfjoin(s, 0.5)
+    assert e.value.status == 4
+
+
+def test_threshold_range(ctx, titles_sets):
+    for t in (0.0, 1.0, -0.5, 1.5):
+        with pytest.raises(F.FgssError) as e:
+            ctx.selfjoin(titles_sets, t)
+        assert e.value.status == 1
+
+
+def test_exact_bounds_equal_rational_brute_force(ctx):
+    rng = np.random.default_rng(9)
+    s = _random_sets(rng, 300, 40, 1, 40)
+    for t, (p, qd) in ((0.8, (4, 5)), (0.6, (3, 5))):
+        got = ctx.selfjoin(s, t, bounds="exact")
+        want = []
+        for qi in range(s.n_sets):
+            x = set(s.tokens[s.pos[qi]:s.pos[qi] + s.len[qi]].tolist())
+            for si in range(qi + 1, s.n_sets):
+                y = set(s.tokens[s.pos[si]:s.pos[si] + s.len[si]].tolist())
+                o = len(x & y)
+                if o and o * qd >= p * (len(x) + len(y) - o):
+                    want.append((qi, si))
+        assert list(zip(got.q.tolist(), got.s.tolist())) == want
+
+
+def test_batch_of_joins_equals_single_joins(ctx):
+    sets = [ctx.tokenize(_titles(n, 100 + n), **datagen.TITLE_TOK) for n in (500, 2500, 1200, 4000)]
+    ts = [0.6, 0.7, 0.9, 0.8]
+    outs = ctx.selfjoin_batch(sets, ts)
+    for s, t, got in zip(sets, ts, outs):
+        ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, t)
+        _check_same(got, ref, st)
+
+
+def test_long_records_take_the_heavy_path(ctx):
+    """Records longer than the shared-memory caps go through the global accumulator."""
+    rng = np.random.default_rng(4)
+    base = rng.choice(8000, size=3000, replace=False)
+    recs = []
+    for i in range(30):
+        r = base.copy()
+        drop = rng.choice(len(r), size=int(rng.integers(0, 300)), replace=False)
+        r = np.delete(r, drop)
+        recs.append(np.sort(r))
+    for i in range(200):
+        recs.append(np.sort(rng.choice(8000, size=int(rng.integers(5, 60)), replace=False)))
+    recs.sort(key=len, reverse=True)
+    lens = np.array([len(r) for r in recs])
+    pos = np.concatenate([[0], np.cumsum(lens[:-1])])
+    s = F.Sets(np.arange(1, len(recs) + 1), pos, lens, np.concatenate(recs), 8000)
+    for method in ("plain", "batched"):
+        got = ctx.selfjoin(s, 0.7, method=method)
+        ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, 0.7)
+        _check_same(got, ref, st)
+        assert got.stats["heavy_queries"] > 0
+
+
+def test_kmer_reads_vs_oracle(ctx):
+    text = datagen.reads(3000, seed=3, genome_len=60000)
+    s = ctx.tokenize(text, **datagen.READ_TOK)
+    for method in ("plain", "batched"):
+        got = ctx.selfjoin(s, 0.8, method=method)
+        ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, 0.8)
+        _check_same(got, ref, st)
