@@ -121,6 +121,7 @@ void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_o
     a.tok = J.in.tokens;
     a.n = (uint32_t)n;
     a.n_terms = v.n_terms;
+    a.n_tokens = v.n_tokens;
     a.status = J.status;
     a.stats = J.stats;
     a.probe = J.lut.probe;
@@ -141,6 +142,14 @@ void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_o
     FGSS_LAUNCH_CK();
     k_send<<<grid_for(kMaxLen + 1, 256), 256, 0, c.stream>>>(J.in.len, (uint32_t)n, J.lut.lmin, send, kMaxLen + 1);
     FGSS_LAUNCH_CK();
+    // no kernel reads tokens through caller offsets before they are validated
+    uint32_t* h = c.pinnedT<uint32_t>(J.pfx("h.prep"), 4);
+    FGSS_CK(cudaMemcpyAsync(h, J.status, 4, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    if (h[0] & ST_BAD_OFFSETS) fail(FGSS_ERR_FORMAT, "a record's pos + len exceeds n_tokens");
+    if (h[0] & ST_TOO_LONG) fail(FGSS_ERR_UNSUPPORTED, "a record has more than 65535 tokens");
+    if (h[0] & ST_BAD_TOKENS)
+        fail(FGSS_ERR_FORMAT, "tokens must be strictly ascending inside each record and below n_terms");
 }
 
 void join_index(Ctx& c, JoinState& J) {

@@ -39,6 +39,7 @@ enum : uint32_t {
     ST_RES_OVERFLOW = 1u << 4,
     ST_HEAVY_OVERFLOW = 1u << 5,
     ST_HASH_FULL = 1u << 6,
+    ST_BAD_OFFSETS = 1u << 7, // a record's pos + len runs past n_tokens
 };
 
 // stats slots (per join, unsigned long long)
@@ -60,6 +61,7 @@ struct JoinArgs {
     const uint32_t* tok;
     uint32_t n;
     uint32_t n_terms;
+    uint64_t n_tokens;
     uint32_t* status;          // ST_* bits
     unsigned long long* stats; // SS_* counters
     // bound tables (bounds.h)
@@ -174,6 +176,12 @@ static __global__ void k_prep(JoinArgs a, uint32_t* __restrict__ icnt, uint32_t*
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t l = a.len[i];
         local_max = max(local_max, l);
+        if ((uint64_t)a.pos[i] + l > a.n_tokens) {
+            bad |= ST_BAD_OFFSETS;
+            icnt[i] = 0;
+            pcnt[i] = 0;
+            continue;
+        }
         if (l > 65535u) {
             bad |= ST_TOO_LONG;
             icnt[i] = 0;
@@ -542,7 +550,8 @@ __device__ void probe_query_smem(const JoinArgs& a, uint32_t q, unsigned char* s
                 my_ver++;
                 if (MODE == MODE_FILL) {
                     uint32_t i = atomicAdd(&s_vc, 1u);
-                    a.cand[a.voff[q] + i] = make_uint4(q, s, c, jm);
+                    if (i < a.vcnt[q]) a.cand[a.voff[q] + i] = make_uint4(q, s, c, jm);
+                    else atomicOr(a.status, ST_HASH_FULL);
                 } else if (MODE == MODE_FUSED) {
                     uint32_t i = atomicAdd(&s_nv, 1u);
                     vl[i] = (uint16_t)h;
@@ -755,7 +764,10 @@ __global__ void __launch_bounds__(NT) k_probe_heavy(const JoinArgs* __restrict__
             if (ub1 >= a.cand_min[S]) my_cand++;
             if (ub1 - 1 >= a.inter_min[S]) {
                 uint32_t v = atomicAdd(&s_nv, 1u);
-                if (MODE == MODE_FILL) a.cand[a.voff[q] + v] = make_uint4(q, s, c, jm);
+                if (MODE == MODE_FILL) {
+                    if (v < a.vcnt[q]) a.cand[a.voff[q] + v] = make_uint4(q, s, c, jm);
+                    else atomicOr(a.status, ST_HASH_FULL);
+                }
                 else if (MODE == MODE_FUSED) gver[v] = s;
             }
         }

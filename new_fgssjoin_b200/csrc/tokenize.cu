@@ -254,13 +254,19 @@ __global__ void k_line_id_keys(const uint32_t* __restrict__ rid, const uint32_t*
 }
 
 // tokens per line (sorted by line): sizes via run boundaries
-__global__ void k_line_sizes(const uint64_t* __restrict__ k2, uint64_t n, uint32_t* __restrict__ lsz,
-                             uint32_t* __restrict__ loff) {
+__global__ void k_line_bounds2(const uint64_t* __restrict__ k2, uint64_t n, uint32_t* __restrict__ lend,
+                               uint32_t* __restrict__ loff) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t l = (uint32_t)(k2[i] >> 32);
         if (i == 0 || (uint32_t)(k2[i - 1] >> 32) != l) loff[l] = (uint32_t)i;
-        if (i + 1 == n || (uint32_t)(k2[i + 1] >> 32) != l) lsz[l] = (uint32_t)(i + 1) - loff[l];
+        if (i + 1 == n || (uint32_t)(k2[i + 1] >> 32) != l) lend[l] = (uint32_t)(i + 1);
     }
+}
+
+__global__ void k_line_sizes(const uint32_t* __restrict__ lend, const uint32_t* __restrict__ loff, uint32_t nlines,
+                             uint32_t* __restrict__ lsz) {
+    for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nlines; l += gridDim.x * blockDim.x)
+        lsz[l] = lend[l] - loff[l];  // both zero for a line without tokens
 }
 
 // record sort keys: lines with tokens, key = (size << 32 | line); value = line
@@ -441,8 +447,12 @@ void tokenize_device(Ctx& c, const char* text, uint64_t n_bytes, const TokParams
     // 6. per-line sizes, records by (size, line)
     uint32_t* lsz = c.devT<uint32_t>("tk.lsz", nlines + 1);
     uint32_t* loff = c.devT<uint32_t>("tk.loff", nlines + 1);
-    FGSS_CK(cudaMemsetAsync(lsz, 0, (uint64_t)nlines * 4, c.stream));
-    k_line_sizes<<<grid_for(Tn, 256, c.num_sms * 32), 256, 0, c.stream>>>(k2, Tn, lsz, loff);
+    uint32_t* lend = c.devT<uint32_t>("tk.lend", nlines + 1);
+    FGSS_CK(cudaMemsetAsync(loff, 0, (uint64_t)nlines * 4, c.stream));
+    FGSS_CK(cudaMemsetAsync(lend, 0, (uint64_t)nlines * 4, c.stream));
+    k_line_bounds2<<<grid_for(Tn, 256, c.num_sms * 32), 256, 0, c.stream>>>(k2, Tn, lend, loff);
+    FGSS_LAUNCH_CK();
+    k_line_sizes<<<grid_for(nlines, 256, c.num_sms * 8), 256, 0, c.stream>>>(lend, loff, nlines, lsz);
     FGSS_LAUNCH_CK();
     k_count_zero<<<grid_for(nlines, 256, c.num_sms * 8), 256, 0, c.stream>>>(lsz, nlines, tot + 5);
     FGSS_LAUNCH_CK();
