@@ -292,7 +292,6 @@ constexpr unsigned long long kEmptySlot = 0xffffffff00000000ull;
 
 // Shared-memory layout of the light-query kernel.
 //   slots u64[H]   (source << 32 | matches << 16 | last query position)
-//   vlist u16[H]   slots that need a merge
 //   wlo/whi u32[kPCap]   full id window of each probe token's list
 //   clo u32[kPCap], wpre u32[kPCap + 4]   the current chunk: first entry, exclusive scan of sizes
 //   qtok u32[kQCap]   query tokens;  bitmap u32[kBmWords] (fused only)
@@ -300,8 +299,7 @@ template <int MODE, int HLOG>
 struct ProbeLayout {
     static constexpr uint32_t H = 1u << HLOG;
     static constexpr uint32_t cap = H / 2;  // window entries per chunk (slot load <= 1/2)
-    static constexpr size_t off_vl = 8ull * H;
-    static constexpr size_t off_wlo = off_vl + 2ull * H;
+    static constexpr size_t off_wlo = 8ull * H;
     static constexpr size_t off_whi = off_wlo + 4ull * kPCap;
     static constexpr size_t off_clo = off_whi + 4ull * kPCap;
     static constexpr size_t off_wpre = off_clo + 4ull * kPCap;
@@ -322,6 +320,18 @@ __device__ __forceinline__ void flush_counters(const JoinArgs& a, const CtaCount
     if (c.verified) atomicAdd(&a.stats[SS_VERIFIED], c.verified);
     if (c.heavy) atomicAdd(&a.stats[SS_HEAVY], c.heavy);
     if (c.merged) atomicAdd(&a.stats[SS_MERGED], c.merged);
+}
+
+// All lanes of a warp: sum the per-thread counters, one lane adds them.
+__device__ __forceinline__ void flush_counters_warp(const JoinArgs& a, CtaCounters c) {
+    c.cand = warp_sum(c.cand);
+    c.inter = warp_sum(c.inter);
+    c.res = warp_sum(c.res);
+    c.window = warp_sum(c.window);
+    c.verified = warp_sum(c.verified);
+    c.heavy = warp_sum(c.heavy);
+    c.merged = warp_sum(c.merged);
+    if (lane_id() == 0) flush_counters(a, c);
 }
 
 // Emits one verified pair (called by one lane).
@@ -406,26 +416,66 @@ __device__ __forceinline__ SlotVerdict slot_verdict(const JoinArgs& a, uint32_t 
     return v;
 }
 
+// Thread-serial merge of a source's tokens from position p0 against the
+// query's term bitmap, counting only tokens above xq (the query token of the
+// last prefix match: everything at or below it was counted by the filter).
+// Stops as soon as c + matches + what can still match < im.
+__device__ __forceinline__ uint32_t thread_merge(const uint32_t* __restrict__ st, uint32_t p0, uint32_t ls,
+                                                 uint32_t xq, uint32_t c, uint32_t qrest, uint32_t im,
+                                                 const uint32_t* bm, bool exact, const uint32_t* qtok, uint32_t qa,
+                                                 uint32_t lq, uint32_t* nread) {
+    uint32_t cnt = c;
+    uint32_t k = p0;
+    auto visit = [&](uint32_t x) {
+        if (x <= xq) return;
+        const uint32_t b = exact ? x : ((x * 0x9E3779B1u) >> 16);
+        bool hit = (bm[b >> 5] >> (b & 31)) & 1u;
+        if (hit && !exact) hit = contains_gen(qtok, qa, lq, x);
+        cnt += hit;
+    };
+    auto alive = [&](uint32_t kk) { return cnt + min(ls - kk, qrest - (cnt - c)) >= im; };
+    bool go = true;
+    while (k < ls && (reinterpret_cast<uintptr_t>(st + k) & 15u)) {
+        if (!alive(k)) { go = false; break; }
+        visit(__ldg(st + k));
+        k++;
+    }
+    while (go && k + 4 <= ls) {
+        if (!alive(k)) { go = false; break; }
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(st + k));
+        visit(v.x);
+        visit(v.y);
+        visit(v.z);
+        visit(v.w);
+        k += 4;
+    }
+    while (go && k < ls) {
+        if (!alive(k)) break;
+        visit(__ldg(st + k));
+        k++;
+    }
+    *nread = k - p0;
+    return cnt;
+}
+
 // Light query on one CTA: shared-memory slot table; the id window is split
 // into chunks of at most `cap` entries (depth-first bisection).  Queries
 // beyond the shared-memory caps go to the heavy queue.
 template <int MODE, int NT, int HLOG>
 __device__ void probe_query_smem(const JoinArgs& a, uint32_t q, unsigned char* smem, CtaCounters& ctr) {
     using Lay = ProbeLayout<MODE, HLOG>;
-    constexpr uint32_t NW = NT / 32;
     unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem);
-    uint16_t* vl = reinterpret_cast<uint16_t*>(smem + Lay::off_vl);
     uint32_t* wlo = reinterpret_cast<uint32_t*>(smem + Lay::off_wlo);
     uint32_t* whi = reinterpret_cast<uint32_t*>(smem + Lay::off_whi);
     uint32_t* clo = reinterpret_cast<uint32_t*>(smem + Lay::off_clo);
     uint32_t* wpre = reinterpret_cast<uint32_t*>(smem + Lay::off_wpre);
     uint32_t* qtok = reinterpret_cast<uint32_t*>(smem + Lay::off_qtok);
     uint32_t* bm = reinterpret_cast<uint32_t*>(smem + Lay::off_bm);
-    __shared__ uint32_t s_L, s_vc, s_nv, s_cand, s_sp, s_win;
+    __shared__ uint32_t s_L, s_vc, s_cand, s_sp, s_win;
     __shared__ uint32_t s_sa[48], s_sb[48];
     __shared__ uint32_t wsum[33];
 
-    const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const uint32_t tid = threadIdx.x, lane = tid & 31;
     const uint32_t st_bits = *a.status;
     if (st_bits & ST_SKIP_ALL) return;
     const uint32_t lq = a.len[q];
@@ -537,8 +587,6 @@ __device__ void probe_query_smem(const JoinArgs& a, uint32_t q, unsigned char* s
         __syncthreads();
         // 4. per slot: reference candidate? needs a merge?
         uint32_t my_cand = 0, my_ver = 0;
-        if (tid == 0) s_nv = 0;
-        __syncthreads();
         for (uint32_t h = tid; h < He; h += NT) {
             const unsigned long long v = slots[h];
             const uint32_t s = (uint32_t)(v >> 32);
@@ -553,8 +601,21 @@ __device__ void probe_query_smem(const JoinArgs& a, uint32_t q, unsigned char* s
                     if (i < a.vcnt[q]) a.cand[a.voff[q] + i] = make_uint4(q, s, c, jm);
                     else atomicOr(a.status, ST_HASH_FULL);
                 } else if (MODE == MODE_FUSED) {
-                    uint32_t i = atomicAdd(&s_nv, 1u);
-                    vl[i] = (uint16_t)h;
+                    // 5. merge right here, one thread per candidate, against the query bitmap
+                    const uint32_t ls = a.len[s], S = lq + ls;
+                    const uint32_t im = a.inter_min[S];
+                    uint32_t nread = 0;
+                    const uint32_t o = thread_merge(a.tok + a.pos[s], c, ls, qtok[jm], c, lq - jm - 1, im, bm,
+                                                    exact_bm, qtok, jm + 1, lq, &nread);
+                    ctr.verified++;
+                    ctr.merged += nread;
+                    if (o >= im && o > 0) {
+                        ctr.inter++;
+                        if (o >= a.need[S]) {
+                            ctr.res++;
+                            emit_result(a, q, s, o);
+                        }
+                    }
                 }
             }
         }
@@ -565,49 +626,6 @@ __device__ void probe_query_smem(const JoinArgs& a, uint32_t q, unsigned char* s
             if (MODE == MODE_COUNT && my_ver) atomicAdd(&s_vc, my_ver);
         }
         __syncthreads();
-        if (MODE == MODE_FUSED) {
-            // 5. merge: warp per candidate; membership through the term bitmap
-            const uint32_t nv = s_nv;
-            for (uint32_t vi = wid; vi < nv; vi += NW) {
-                const unsigned long long v = slots[vl[vi]];
-                const uint32_t s = (uint32_t)(v >> 32);
-                const uint32_t c = ((uint32_t)v >> 16) & 0xffffu, jm = (uint32_t)v & 0xffffu;
-                const uint32_t ls = a.len[s], S = lq + ls;
-                const uint32_t im = a.inter_min[S];
-                const uint32_t* st = a.tok + a.pos[s];
-                const uint32_t smx = warp_find(st, a.index[ls], qtok[jm]);
-                uint32_t cnt = c;
-                const uint32_t qrest = lq - jm - 1;
-                uint32_t bend = smx + 1;
-                for (uint32_t b = smx + 1; b < ls; b += 32) {
-                    bend = min(b + 32, ls);
-                    const uint32_t k = b + lane;
-                    bool hit = false;
-                    if (k < ls) {
-                        const uint32_t x = __ldg(st + k);
-                        const uint32_t bb = exact_bm ? x : ((x * 0x9E3779B1u) >> 16);
-                        hit = (bm[bb >> 5] >> (bb & 31)) & 1u;
-                        if (hit && !exact_bm) hit = contains_gen(qtok, jm + 1, lq, x);
-                    }
-                    cnt += __popc(__ballot_sync(kFull, hit));
-                    const uint32_t rs = ls > b + 32 ? ls - b - 32 : 0;
-                    const uint32_t rq = qrest - (cnt - c);
-                    if (cnt + min(rs, rq) < im) break;
-                }
-                if (lane == 0) {
-                    ctr.verified++;
-                    ctr.merged += bend;  // index-prefix search + merged suffix of the source
-                    if (cnt >= im && cnt > 0) {
-                        ctr.inter++;
-                        if (cnt >= a.need[S]) {
-                            ctr.res++;
-                            emit_result(a, q, s, cnt);
-                        }
-                    }
-                }
-            }
-            __syncthreads();
-        }
         // 6. clear the slots of this chunk
         for (uint32_t h = tid; h < He; h += NT) slots[h] = kEmptySlot;
     }
@@ -651,7 +669,7 @@ __global__ void __launch_bounds__(NT) k_probe(const JoinArgs* __restrict__ joins
     if (items == nullptr) {
         const JoinArgs& a = joins[0];
         probe_query_smem<MODE, NT, HLOG>(a, blockIdx.x, smem, ctr);
-        if (MODE == MODE_FUSED && (threadIdx.x & 31) == 0) flush_counters(a, ctr);
+        if (MODE == MODE_FUSED) flush_counters_warp(a, ctr);
         return;
     }
     __shared__ uint32_t s_item;
@@ -664,14 +682,14 @@ __global__ void __launch_bounds__(NT) k_probe(const JoinArgs* __restrict__ joins
         if (it >= n_items) break;
         const uint4 w = items[it];
         if (w.x != cur_join) {
-            if (cur_join != 0xffffffffu && (threadIdx.x & 31) == 0) flush_counters(joins[cur_join], ctr);
+            if (cur_join != 0xffffffffu) flush_counters_warp(joins[cur_join], ctr);
             ctr = {0, 0, 0, 0, 0, 0, 0};
             cur_join = w.x;
         }
         const JoinArgs& a = joins[w.x];
         for (uint32_t q = w.y; q < w.z; q++) probe_query_smem<MODE, NT, HLOG>(a, q, smem, ctr);
     }
-    if (cur_join != 0xffffffffu && (threadIdx.x & 31) == 0) flush_counters(joins[cur_join], ctr);
+    if (cur_join != 0xffffffffu) flush_counters_warp(joins[cur_join], ctr);
 }
 
 // ------------------------------------------------------------ heavy queries

@@ -20,7 +20,9 @@ def test_exclusive_scan(ctx, n):
 @pytest.mark.parametrize("n,bits", [(1, 8), (1000, 13), (70000, 64), (1_000_003, 40)])
 def test_radix_sort_stable(ctx, n, bits):
     rng = np.random.default_rng(bits)
-    k = rng.integers(0, 2 ** min(bits, 63), n, dtype=np.uint64) & np.uint64((1 << bits) - 1 if bits < 64 else ~0)
+    k = rng.integers(0, 2 ** 63, n, dtype=np.uint64) * np.uint64(2) + rng.integers(0, 2, n, dtype=np.uint64)
+    if bits < 64:
+        k &= np.uint64((1 << bits) - 1)
     k[::7] = k[0]  # duplicates to exercise stability
     v = np.arange(n, dtype=np.uint32)
     dk = torch.from_numpy(k.view(np.int64)).cuda()
