@@ -146,6 +146,8 @@ typedef struct fgss_join_opts {
     int out_on_device;      /* 1 = pairs stay in device memory (library-owned) */
     int want_candidates;    /* 1 = also return the candidate list (debug / tests) */
     int use_model;          /* batched method: presize and bin with the learned model */
+    uint64_t result_capacity; /* batched method: presized result slots; 0 = learned / automatic.
+                                 Too small a value only costs an exact re-run. */
 } fgss_join_opts;
 
 void fgss_join_opts_default(fgss_join_opts* o);
@@ -211,6 +213,12 @@ fgss_status fgss_pairs_print(const fgss_pairs* p, void* file);
 fgss_status fgss_model_train(fgss_ctx* ctx, const fgss_sets_view* sets, const float* thresholds,
                              int n, int epochs, float lr, uint64_t seed, float* final_loss);
 fgss_status fgss_model_save(fgss_ctx* ctx, const char* path);
+/* One forward + backward pass of the MLP on host arrays (n x 8 features,
+ * n x 2 targets), for gradient checks: params (354 floats) -> grads, loss. */
+fgss_status fgss_model_grad(fgss_ctx* ctx, const float* feat, const float* target, uint64_t n, const float* params,
+                            float* grads, float* loss);
+/* Number of MLP parameters (W1, b1, W2, b2). */
+int fgss_model_num_params(void);
 fgss_status fgss_model_load(fgss_ctx* ctx, const char* path);
 
 /* Host-side bound tables of one threshold (no device needed): for lengths

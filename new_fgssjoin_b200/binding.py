@@ -17,7 +17,7 @@ EXPORTED_SYMBOLS = [
     "fgss_load_bin", "fgss_write_bin", "fgss_sets_free", "fgss_sets_view_of",
     "fgss_tok_opts_default", "fgss_tokenize",
     "fgss_join_opts_default", "fgss_selfjoin", "fgss_selfjoin_batch", "fgss_pairs_free", "fgss_pairs_print",
-    "fgss_model_train", "fgss_model_save", "fgss_model_load",
+    "fgss_model_train", "fgss_model_save", "fgss_model_load", "fgss_model_grad", "fgss_model_num_params",
     "fgss_bounds_table", "fgss_dev_exclusive_scan_u32", "fgss_dev_sort_pairs_u64",
 ]
 
@@ -48,7 +48,8 @@ class _TokOpts(ctypes.Structure):
 
 class _JoinOpts(ctypes.Structure):
     _fields_ = [("threshold", ctypes.c_float), ("bounds", ctypes.c_int), ("method", ctypes.c_int),
-                ("out_on_device", ctypes.c_int), ("want_candidates", ctypes.c_int), ("use_model", ctypes.c_int)]
+                ("out_on_device", ctypes.c_int), ("want_candidates", ctypes.c_int), ("use_model", ctypes.c_int),
+                ("result_capacity", ctypes.c_uint64)]
 
 
 class _Stats(ctypes.Structure):
@@ -106,6 +107,8 @@ def load_library():
                                    ctypes.c_float, ctypes.c_uint64, P(ctypes.c_float)]
     L.fgss_model_save.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
     L.fgss_model_load.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+    L.fgss_model_grad.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                  ctypes.c_void_p, P(ctypes.c_float)]
     L.fgss_dev_exclusive_scan_u32.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64]
     L.fgss_dev_sort_pairs_u64.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                           ctypes.c_int, ctypes.c_int]
@@ -292,7 +295,7 @@ class Context:
 
     # ----------------------------------------------------------------- join
     @staticmethod
-    def _opts(threshold, method, bounds, want_candidates, use_model, out_on_device=False):
+    def _opts(threshold, method, bounds, want_candidates, use_model, out_on_device=False, result_capacity=0):
         o = _JoinOpts()
         o.threshold = float(threshold)
         o.method = {"plain": METHOD_PLAIN, "batched": METHOD_BATCHED}.get(method, method)
@@ -300,6 +303,7 @@ class Context:
         o.want_candidates = int(want_candidates)
         o.use_model = int(use_model)
         o.out_on_device = int(out_on_device)
+        o.result_capacity = int(result_capacity)
         return o
 
     def _collect(self, p, st, want_candidates):
@@ -319,10 +323,10 @@ class Context:
         return out
 
     def selfjoin(self, sets, threshold, method="plain", bounds="reference", want_candidates=False,
-                 use_model=False):
+                 use_model=False, result_capacity=0):
         """Self-join of ``sets`` (host Sets or a device view) at ``threshold``."""
         v = sets.view() if isinstance(sets, Sets) else sets
-        o = self._opts(threshold, method, bounds, want_candidates, use_model)
+        o = self._opts(threshold, method, bounds, want_candidates, use_model, result_capacity=result_capacity)
         p = _Pairs()
         st = _Stats()
         rc = self._L.fgss_selfjoin(self._ctx, ctypes.byref(v), ctypes.byref(o), ctypes.byref(p), ctypes.byref(st))
@@ -349,6 +353,18 @@ class Context:
         rc = self._L.fgss_model_train(self._ctx, views, ts, n, epochs, lr, seed, ctypes.byref(loss))
         _check(self._L, self._ctx, rc)
         return float(loss.value)
+
+    def model_grad(self, feat, target, params):
+        """One GPU forward/backward of the cost-model MLP: returns (grads, loss)."""
+        feat = np.ascontiguousarray(feat, np.float32)
+        target = np.ascontiguousarray(target, np.float32)
+        params = np.ascontiguousarray(params, np.float32)
+        grads = np.zeros_like(params)
+        loss = ctypes.c_float()
+        rc = self._L.fgss_model_grad(self._ctx, feat.ctypes.data, target.ctypes.data, feat.shape[0],
+                                     params.ctypes.data, grads.ctypes.data, ctypes.byref(loss))
+        _check(self._L, self._ctx, rc)
+        return grads, float(loss.value)
 
     def model_save(self, path):
         _check(self._L, self._ctx, self._L.fgss_model_save(self._ctx, os.fsencode(path)))

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 
+#include "fused_kernels.cuh"
 #include "join.h"
 #include "model.h"
 #include "prims.cuh"
@@ -74,38 +75,52 @@ __global__ void k_items(const uint32_t* __restrict__ pre, uint32_t n, uint64_t t
 }
 
 template <int NT, int HLOG>
-static void launch_fused(Ctx& c, const JoinArgs* d_args, const uint4* items, uint32_t n_items, uint32_t* counter,
-                         int ctas_per_sm) {
+static void launch_fused(Ctx& c, const JoinArgs* d_args, const FusedArgs* d_fargs, const uint4* items,
+                         uint32_t n_items, uint32_t* counter, int ctas_per_sm) {
     static bool attr = false;
-    const size_t smem = ProbeLayout<MODE_FUSED, HLOG>::bytes;
+    const size_t smem = FusedLayout<HLOG>::bytes;
     if (!attr) {
-        FGSS_CK(cudaFuncSetAttribute(k_probe<MODE_FUSED, NT, HLOG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
+        FGSS_CK(cudaFuncSetAttribute(k_fused<NT, HLOG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
     int occ = 0;
-    FGSS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_probe<MODE_FUSED, NT, HLOG>, NT, smem));
+    FGSS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused<NT, HLOG>, NT, smem));
     if (occ < 1) occ = 1;
-    int per = std::min(occ, std::max(1, ctas_per_sm));
-    unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)per * c.num_sms, std::max<uint32_t>(n_items, 1));
-    k_probe<MODE_FUSED, NT, HLOG><<<grid, NT, smem, c.stream>>>(d_args, items, n_items, counter);
+    const int per = ctas_per_sm > 0 ? std::min(occ, ctas_per_sm) : occ;
+    const unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)per * c.num_sms, std::max<uint32_t>(n_items, 1));
+    k_fused<NT, HLOG><<<grid, NT, smem, c.stream>>>(d_args, d_fargs, items, n_items, counter);
     FGSS_LAUNCH_CK();
 }
 
-void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const uint4* items, uint32_t n_items,
-                  uint32_t* counter) {
-#define FGSS_F(NT, HL)                                                            \
-    if (te.threads == NT && te.hash_log2 == HL) {                                 \
-        launch_fused<NT, HL>(c, d_args, items, n_items, counter, te.ctas_per_sm); \
-        return;                                                                   \
+// Launch shapes the autotuner chooses from.
+const int kFusedShapes[][2] = {{128, 10}, {128, 11}, {256, 11}, {256, 12}, {512, 12}, {512, 13}};
+const int kNumFusedShapes = 6;
+
+void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const FusedArgs* d_fargs, const uint4* items,
+                  uint32_t n_items, uint32_t* counter) {
+#define FGSS_F(NT, HL)                                                                     \
+    if (te.threads == NT && te.hash_log2 == HL) {                                          \
+        launch_fused<NT, HL>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm); \
+        return;                                                                            \
     }
+    FGSS_F(128, 10)
+    FGSS_F(128, 11)
+    FGSS_F(256, 11)
     FGSS_F(256, 12)
-    FGSS_F(256, 13)
     FGSS_F(512, 12)
     FGSS_F(512, 13)
-    FGSS_F(512, 14)
 #undef FGSS_F
-    launch_fused<256, 12>(c, d_args, items, n_items, counter, te.ctas_per_sm);
+    launch_fused<256, 11>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm);
+}
+
+// Work-item cost of a query: exact window entries + a verification estimate.
+__global__ void k_cost(const uint32_t* __restrict__ wtot, const uint32_t* __restrict__ len,
+                       const uint32_t* __restrict__ pred_cand, uint32_t n, uint32_t* __restrict__ cost) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        unsigned long long v = (unsigned long long)wtot[q] + len[q];
+        if (pred_cand) v += 4ull * pred_cand[q];
+        cost[q] = (uint32_t)min(v, 0x3fffffffull);
+    }
 }
 
 // Resets the filter's counters and overflow bit of one join before a re-run
@@ -125,20 +140,40 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
     uint64_t* d_tot = c.devT<uint64_t>("b.tot", nj * 2 + 2);
     std::vector<uint32_t*> pre(nj);
     FGSS_CK(cudaMemsetAsync(d_tot, 0, (nj * 2 + 2) * 8, c.stream));
+    std::vector<FusedArgs> hf(nj);
     for (size_t i = 0; i < nj; i++) {
         JoinState& J = *joins[i];
         const uint64_t n = J.in.n_sets;
         float* feat = c.devT<float>(J.pfx("feat"), (n + 1) * kFeat);
         uint32_t* cost = c.devT<uint32_t>(J.pfx("cost"), n + 1);
+        uint32_t* fcost = c.devT<uint32_t>(J.pfx("fcost"), n + 1);
+        uint32_t* poff = c.devT<uint32_t>(J.pfx("poff"), n + 1);
+        uint2* win = c.devT<uint2>(J.pfx("win"), J.in.n_tokens + 1);
+        uint32_t* wtot = c.devT<uint32_t>(J.pfx("wtot"), n + 1);
+        uint32_t* pred = c.devT<uint32_t>(J.pfx("pred"), n + 1);
         pre[i] = c.devT<uint32_t>(J.pfx("cpre"), n + 1);
+        hf[i].poff = poff;
+        hf[i].win = win;
+        hf[i].smin = J.lut.smin;
         if (n == 0) continue;
-        k_features<<<grid_for(n * 32, 256, c.num_sms * 32), 256, 0, c.stream>>>(J.args, J.t, feat, cost);
+        // windows of every probe token (exact per-query work), then features and the learned estimate
+        exclusive_scan<uint32_t>(c, J.pcnt, poff, n, nullptr, (uint32_t*)nullptr, J.pfx("scan.p").c_str());
+        k_windows<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wtot);
         FGSS_LAUNCH_CK();
-        if (use_model && c.model) model_predict(c, feat, n, cost, &d_tot[nj + i]);
+        const bool model = use_model && c.model && !J.res_cap_hint;
+        if (model) {
+            k_features<<<grid_for(n * 32, 256, c.num_sms * 32), 256, 0, c.stream>>>(J.args, J.t, feat, fcost);
+            FGSS_LAUNCH_CK();
+            model_predict(c, feat, n, pred, &d_tot[nj + i]);
+        }
+        k_cost<<<grid_for(n, 256, c.num_sms * 8), 256, 0, c.stream>>>(wtot, J.in.len, model ? pred : nullptr,
+                                                                       (uint32_t)n, cost);
+        FGSS_LAUNCH_CK();
         exclusive_scan<uint32_t>(c, cost, pre[i], n, nullptr, (uint32_t*)nullptr, J.pfx("scan.cost").c_str());
-        // total cost (64-bit)
         model_sum_cost(c, cost, n, &d_tot[i]);
     }
+    FusedArgs* d_fargs = c.devT<FusedArgs>("b.fargs", nj);
+    FGSS_CK(cudaMemcpyAsync(d_fargs, hf.data(), nj * sizeof(FusedArgs), cudaMemcpyHostToDevice, c.stream));
     std::vector<uint64_t> htot(2 * nj + 2);
     FGSS_CK(cudaMemcpyAsync(htot.data(), d_tot, (2 * nj + 2) * 8, cudaMemcpyDeviceToHost, c.stream));
     c.sync();
@@ -179,7 +214,10 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         const uint64_t last = itc != c.tune.end() ? (uint64_t)itc->second.ctas_per_sm : 0;
         if (J.res_cap_hint) {
             cap = J.res_cap_hint;
+        } else if (J.res_cap_user) {
+            cap = J.res_cap_user;
         } else if (use_model && c.model) {
+            // the model's predicted result count, x1.5 + slack
             cap = (uint64_t)((double)htot[nj + i] * 1.5) + 4096;  // predicted results x 1.5 + slack
         } else {
             cap = std::max<uint64_t>(n + 4096, last);
@@ -198,7 +236,7 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
     uint32_t* counter = c.devT<uint32_t>("b.counter", 4 + nj);
     FGSS_CK(cudaMemsetAsync(counter, 0, (4 + nj) * 4, c.stream));
     FGSS_CK(cudaEventRecord(c.ev[4], c.stream));
-    if (nitems) fused_launch(c, te, d_args, items, (uint32_t)nitems, counter);
+    if (nitems) fused_launch(c, te, d_args, d_fargs, items, (uint32_t)nitems, counter);
     FGSS_CK(cudaEventRecord(c.ev[5], c.stream));
     c.probe_timed = true;
     // heavy queries: read the queue sizes, one persistent launch per join

@@ -1,0 +1,351 @@
+// fused_kernels.cuh -- the batched method's filter + verify kernel.
+//
+// Same semantics as the plain stages (join_kernels.cuh; reference
+// filtering.cu:76-141, checking.cu:93-175, block.cu:184-197), organised for
+// throughput:
+//   * k_windows: one warp per query computes the id window [q+1, send) of
+//     every probe token's list by binary search, for all queries at once
+//     (massively parallel, latency hidden by occupancy), and the per-query
+//     window total that sizes work items.
+//   * k_fused: persistent CTAs pull work items (runs of queries of one join).
+//     Per query: the query's tokens and term bitmap go to shared memory, the
+//     precomputed windows are read with one coalesced load, window entries are
+//     accumulated into a shared-memory slot table (64-bit CAS per entry) that
+//     also appends every newly occupied slot to a list, and a lane-persistent
+//     loop drains that list: each lane takes the next slot, decides whether it
+//     is a reference candidate and whether a merge can still reach floor(min
+//     overlap), then merges the source's tokens 16 bytes per step against the
+//     query bitmap, taking the next slot as soon as it is done.  Lanes stay
+//     converged on the same short loop body instead of diverging over
+//     candidates of different lengths.
+#pragma once
+
+#include "join_kernels.cuh"
+
+namespace fgss {
+
+// Layout: slots u64[H] | occ u16[H] | wlo,whi,clo u32[PC] | wpre u32[PC+4] | qtok u32[QC] | bm u32[BW]
+template <int HLOG>
+struct FusedLayout {
+    static constexpr uint32_t H = 1u << HLOG;
+    static constexpr uint32_t cap = H / 2;    // window entries per chunk
+    static constexpr uint32_t PC = H / 4;     // probe tokens handled in shared memory
+    static constexpr uint32_t QC = H / 2;     // query tokens staged in shared memory
+    static constexpr uint32_t BW = 1024;      // bitmap words: 32768 bits
+    static constexpr size_t off_occ = 8ull * H;
+    static constexpr size_t off_wlo = off_occ + 2ull * H;
+    static constexpr size_t off_whi = off_wlo + 4ull * PC;
+    static constexpr size_t off_clo = off_whi + 4ull * PC;
+    static constexpr size_t off_wpre = off_clo + 4ull * PC;
+    static constexpr size_t off_qtok = off_wpre + 4ull * (PC + 4);
+    static constexpr size_t off_bm = off_qtok + 4ull * QC;
+    static constexpr size_t bytes = off_bm + 4ull * BW;
+};
+
+// Window of every probe token: warp per query.  win[poff[q] + j] = (lo, hi);
+// wtot[q] = sum of the window sizes.
+static __global__ void k_windows(JoinArgs a, const uint32_t* __restrict__ poff, uint2* __restrict__ win,
+                                 uint32_t* __restrict__ wtot) {
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t lane = lane_id();
+    const bool unsorted = (*a.status & ST_UNSORTED) != 0;
+    for (uint32_t q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < a.n; q += warps) {
+        const uint32_t lq = a.len[q];
+        const uint32_t qp = lq <= 65535u ? a.probe[lq] : 0;
+        const uint32_t send = unsorted ? a.n : (lq <= 65535u ? a.send[lq] : 0);
+        const uint32_t* qt = a.tok + a.pos[q];
+        const uint32_t o = poff[q];
+        uint32_t tot = 0;
+        for (uint32_t j = lane; j < qp; j += 32) {
+            const uint32_t w = __ldg(qt + j);
+            const uint32_t b = __ldg(a.list_off + w), e = __ldg(a.list_off + w + 1);
+            uint32_t lo = e, hi = e;
+            if (send > q + 1) {
+                lo = lower_bound_u32(a.ent_s, b, e, q + 1);
+                hi = unsorted ? e : lower_bound_u32(a.ent_s, lo, e, send);
+            }
+            win[o + j] = make_uint2(lo, hi);
+            tot += hi - lo;
+        }
+        tot = warp_sum(tot);
+        if (lane == 0) wtot[q] = tot;
+    }
+}
+
+struct FusedArgs {
+    const uint32_t* poff;  // per query: first probe window
+    const uint2* win;
+    const uint4* smin;     // per length sum S: (cand_min, inter_min, need, 0)
+};
+
+__device__ __forceinline__ bool bm_test(const uint32_t* bm, bool exact, uint32_t x, const uint32_t* qtok, uint32_t qa,
+                                        uint32_t lq) {
+    const uint32_t b = exact ? x : ((x * 0x9E3779B1u) >> 17);
+    bool hit = (bm[b >> 5] >> (b & 31)) & 1u;
+    if (hit && !exact) hit = contains_gen(qtok, qa, lq, x);
+    return hit;
+}
+
+template <int NT, int HLOG>
+__device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, unsigned char* smem,
+                            CtaCounters& ctr) {
+    using Lay = FusedLayout<HLOG>;
+    unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem);
+    uint16_t* occ = reinterpret_cast<uint16_t*>(smem + Lay::off_occ);
+    uint32_t* wlo = reinterpret_cast<uint32_t*>(smem + Lay::off_wlo);
+    uint32_t* whi = reinterpret_cast<uint32_t*>(smem + Lay::off_whi);
+    uint32_t* clo = reinterpret_cast<uint32_t*>(smem + Lay::off_clo);
+    uint32_t* wpre = reinterpret_cast<uint32_t*>(smem + Lay::off_wpre);
+    uint32_t* qtok = reinterpret_cast<uint32_t*>(smem + Lay::off_qtok);
+    uint32_t* bm = reinterpret_cast<uint32_t*>(smem + Lay::off_bm);
+    __shared__ uint32_t s_L, s_sp, s_nocc, s_next, s_cand, s_win;
+    __shared__ uint32_t s_sa[48], s_sb[48];
+    __shared__ uint32_t wsum[33];
+
+    const uint32_t tid = threadIdx.x, lane = tid & 31;
+    const uint32_t st_bits = *a.status;
+    if (st_bits & ST_SKIP_ALL) return;
+    const uint32_t lq = a.len[q];
+    if (lq == 0 || lq > 65535u) return;
+    const uint32_t qp = a.probe[lq];
+    if (qp == 0) return;
+    const bool unsorted = (st_bits & ST_UNSORTED) != 0;
+    const uint32_t send = unsorted ? a.n : a.send[lq];
+    if (send <= q + 1) return;
+    if (qp > Lay::PC || lq > Lay::QC) {
+        if (tid == 0) defer_heavy(a, q);
+        return;
+    }
+    const bool exact_bm = a.n_terms <= Lay::BW * 32;
+    const uint32_t* qt = a.tok + a.pos[q];
+    const uint2* qwin = fa.win + fa.poff[q];
+    for (uint32_t j = tid; j < lq; j += NT) {
+        const uint32_t x = __ldg(qt + j);
+        qtok[j] = x;
+        const uint32_t b = exact_bm ? x : ((x * 0x9E3779B1u) >> 17);
+        atomicOr(&bm[b >> 5], 1u << (b & 31));
+    }
+    for (uint32_t j = tid; j < qp; j += NT) {
+        const uint2 w = qwin[j];
+        wlo[j] = w.x;
+        whi[j] = w.y;
+    }
+    if (tid == 0) {
+        s_cand = 0;
+        s_win = 0;
+        s_sp = 1;
+        s_sa[0] = q + 1;
+        s_sb[0] = send;
+    }
+    for (;;) {
+        __syncthreads();
+        const uint32_t sp = s_sp;
+        if (sp == 0) break;
+        const uint32_t ra = s_sa[sp - 1], rb = s_sb[sp - 1];
+        {
+            constexpr uint32_t PER = (Lay::PC + NT - 1) / NT;
+            const uint32_t b0 = tid * PER;
+            uint32_t loc[PER];
+            uint32_t sum = 0;
+#pragma unroll
+            for (uint32_t i = 0; i < PER; i++) {
+                const uint32_t j = b0 + i;
+                uint32_t cnt = 0;
+                if (j < qp) {
+                    const uint32_t lo0 = wlo[j], hi0 = whi[j];
+                    const uint32_t lo = (ra == q + 1) ? lo0 : lower_bound_u32(a.ent_s, lo0, hi0, ra);
+                    const uint32_t hi = (rb == send) ? hi0 : lower_bound_u32(a.ent_s, lo, hi0, rb);
+                    cnt = hi - lo;
+                    clo[j] = lo;
+                }
+                loc[i] = cnt;
+                sum += cnt;
+            }
+            uint32_t tot;
+            uint32_t pre = block_excl_scan<uint32_t>(sum, wsum, &tot);
+#pragma unroll
+            for (uint32_t i = 0; i < PER; i++) {
+                const uint32_t j = b0 + i;
+                if (j < qp) wpre[j] = pre;
+                pre += loc[i];
+            }
+            if (tid == 0) {
+                wpre[qp] = tot;
+                s_L = tot;
+                s_nocc = 0;
+                s_next = 0;
+            }
+        }
+        __syncthreads();
+        const uint32_t L = s_L;
+        if (L > Lay::cap && rb - ra > 1) {
+            if (tid == 0) {
+                const uint32_t mid = ra + (rb - ra) / 2;
+                s_sa[sp - 1] = mid;
+                s_sb[sp - 1] = rb;
+                s_sa[sp] = ra;
+                s_sb[sp] = mid;
+                s_sp = sp + 1;
+            }
+            continue;
+        }
+        if (tid == 0) {
+            s_sp = sp - 1;
+            s_win += L;
+        }
+        if (L == 0) continue;
+        int hl = 6;
+        while ((1u << hl) < 2 * L && hl < HLOG) hl++;
+        const uint32_t mask = (1u << hl) - 1;
+        // accumulate; a newly occupied slot goes on the occupied list
+        for (uint32_t f = tid; f < L; f += NT) {
+            const uint32_t j = upper_bound_gen(wpre, 0, qp, f) - 1;
+            const uint32_t k = clo[j] + (f - wpre[j]);
+            const uint32_t s = __ldg(a.ent_s + k);
+            if (unsorted && !size_ok(a, lq, a.len[s])) continue;
+            uint32_t h = hash_slot(s, hl);
+            bool done = false;
+            for (uint32_t it = 0; it <= mask && !done; it++) {
+                unsigned long long old = *(volatile unsigned long long*)&slots[h];
+                for (;;) {
+                    const uint32_t key = (uint32_t)(old >> 32);
+                    unsigned long long nw;
+                    if (key == s) {
+                        const uint32_t lo = (uint32_t)old;
+                        nw = ((unsigned long long)s << 32) | ((((lo >> 16) + 1u) << 16) | max(lo & 0xffffu, j));
+                    } else if (key == kEmpty) {
+                        nw = ((unsigned long long)s << 32) | ((1u << 16) | j);
+                    } else {
+                        break;
+                    }
+                    const unsigned long long prev = atomicCAS(&slots[h], old, nw);
+                    if (prev == old) {
+                        if (key == kEmpty) occ[atomicAdd(&s_nocc, 1u)] = (uint16_t)h;
+                        done = true;
+                        break;
+                    }
+                    old = prev;
+                }
+                if (!done) h = (h + 1) & mask;
+            }
+            if (!done) atomicOr(a.status, ST_HASH_FULL);
+        }
+        __syncthreads();
+        // lane-persistent decide + merge over the occupied slots
+        const uint32_t nocc = s_nocc;
+        uint32_t my_cand = 0;
+        bool have = false;
+        uint32_t s = 0, c = 0, xq = 0, ls = 0, k = 0, cnt = 0, qrest = 0, im = 0, need = 0, p0 = 0;
+        const uint32_t* st = nullptr;
+        auto tally = [&](uint32_t o, uint32_t kend) {
+            ctr.verified++;
+            ctr.merged += kend - p0;
+            if (o >= im && o > 0) {
+                ctr.inter++;
+                if (o >= need) {
+                    ctr.res++;
+                    emit_result(a, q, s, o);
+                }
+            }
+        };
+        for (;;) {
+            if (!have) {
+                const uint32_t i = atomicAdd(&s_next, 1u);
+                if (i >= nocc) break;
+                const unsigned long long v = slots[occ[i]];
+                s = (uint32_t)(v >> 32);
+                c = ((uint32_t)v >> 16) & 0xffffu;
+                const uint32_t jm = (uint32_t)v & 0xffffu;
+                ls = a.len[s];
+                st = a.tok + a.pos[s];
+                const uint4 sm = fa.smin[lq + ls];
+                const uint32_t ips = a.index[ls];
+                xq = qtok[jm];
+                const uint32_t A = lq - jm;
+                const bool cand = (c + A >= sm.x) && smax_le(st, (int)ls + (int)c - (int)sm.x, c, ips, xq);
+                const bool ver = (c + A - 1 >= sm.y) && smax_le(st, (int)ls + (int)c - 1 - (int)sm.y, c, ips, xq);
+                my_cand += cand;
+                if (!ver) continue;
+                im = sm.y;
+                need = sm.z;
+                qrest = lq - jm - 1;
+                cnt = c;
+                k = c;  // the last match sits at or after position c - 1
+                p0 = k;
+                if (k >= ls || cnt + min(ls - k, qrest) < im) {
+                    tally(c, k);
+                    continue;
+                }
+                have = true;
+            }
+            // one 16-byte step of the merge
+            const uintptr_t addr = reinterpret_cast<uintptr_t>(st + k);
+            const uint4 v4 = __ldg(reinterpret_cast<const uint4*>(addr & ~uintptr_t(15)));
+            const uint32_t off = (uint32_t)(addr & 15u) >> 2;
+            const uint32_t n_in = min(4u - off, ls - k);
+            const uint32_t xs[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+            for (uint32_t t = 0; t < 4; t++) {
+                if (t >= off && t < off + n_in) {
+                    const uint32_t x = xs[t];
+                    if (x > xq && bm_test(bm, exact_bm, x, qtok, 0, lq)) cnt++;
+                }
+            }
+            k += n_in;
+            if (k >= ls || cnt + min(ls - k, qrest - (cnt - c)) < im) {
+                have = false;
+                tally(cnt, k);
+            }
+        }
+        my_cand = warp_sum(my_cand);
+        if (lane == 0 && my_cand) atomicAdd(&s_cand, my_cand);
+        __syncthreads();
+        for (uint32_t i = tid; i < nocc; i += NT) slots[occ[i]] = kEmptySlot;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        ctr.cand += s_cand;
+        ctr.window += s_win;
+    }
+    for (uint32_t j = tid; j < lq; j += NT) {
+        const uint32_t x = qtok[j];
+        const uint32_t b = exact_bm ? x : ((x * 0x9E3779B1u) >> 17);
+        bm[b >> 5] = 0u;
+    }
+    __syncthreads();
+}
+
+template <int NT, int HLOG>
+__global__ void __launch_bounds__(NT) k_fused(const JoinArgs* __restrict__ joins, const FusedArgs* __restrict__ fargs,
+                                              const uint4* __restrict__ items, uint32_t n_items,
+                                              uint32_t* item_counter) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    using Lay = FusedLayout<HLOG>;
+    unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem);
+    uint32_t* bm = reinterpret_cast<uint32_t*>(smem + Lay::off_bm);
+    for (uint32_t h = threadIdx.x; h < Lay::H; h += NT) slots[h] = kEmptySlot;
+    for (uint32_t i = threadIdx.x; i < Lay::BW; i += NT) bm[i] = 0u;
+    __syncthreads();
+    CtaCounters ctr = {0, 0, 0, 0, 0, 0, 0};
+    __shared__ uint32_t s_item;
+    uint32_t cur_join = 0xffffffffu;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(item_counter, 1u);
+        __syncthreads();
+        const uint32_t it = s_item;
+        __syncthreads();
+        if (it >= n_items) break;
+        const uint4 w = items[it];
+        if (w.x != cur_join) {
+            if (cur_join != 0xffffffffu) flush_counters_warp(joins[cur_join], ctr);
+            ctr = {0, 0, 0, 0, 0, 0, 0};
+            cur_join = w.x;
+        }
+        const JoinArgs& a = joins[w.x];
+        const FusedArgs& fa = fargs[w.x];
+        for (uint32_t q = w.y; q < w.z; q++) fused_query<NT, HLOG>(a, fa, q, smem, ctr);
+    }
+    if (cur_join != 0xffffffffu) flush_counters_warp(joins[cur_join], ctr);
+}
+
+}  // namespace fgss

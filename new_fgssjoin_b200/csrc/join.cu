@@ -59,6 +59,7 @@ DevBounds device_bounds(Ctx& c, float t, int mode) {
     d.cand_min = c.devT<uint32_t>(k + "cand", S);
     d.inter_min = c.devT<uint32_t>(k + "inter", S);
     d.need = c.devT<uint32_t>(k + "need", S);
+    d.smin = c.devT<uint4>(k + "smin", S);
     if (fresh) {
         BoundTables b;
         compute_bounds(t, mode, b);
@@ -70,6 +71,9 @@ DevBounds device_bounds(Ctx& c, float t, int mode) {
         upload(c, d.cand_min, b.cand_min);
         upload(c, d.inter_min, b.inter_min);
         upload(c, d.need, b.need);
+        std::vector<uint4> sm(S);
+        for (size_t i = 0; i < S; i++) sm[i] = make_uint4(b.cand_min[i], b.inter_min[i], b.need[i], 0u);
+        upload(c, d.smin, sm);
         c.sync();  // the host vectors go out of scope
     }
     return d;
@@ -78,6 +82,7 @@ DevBounds device_bounds(Ctx& c, float t, int mode) {
 void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_opts& o, int slot) {
     J.slot = slot;
     J.t = o.threshold;
+    J.res_cap_user = o.result_capacity;
     J.bounds = o.bounds;
     if (!(o.threshold > 0.0f && o.threshold < 1.0f))
         fail(FGSS_ERR_INVALID, "threshold must be in (0, 1) (fgssjoin_cli.cu:31-35)");

@@ -19,6 +19,7 @@ struct DevBounds {
     uint32_t* cand_min;
     uint32_t* inter_min;
     uint32_t* need;
+    uint4* smin;  // per length sum: (cand_min, inter_min, need, 0)
 };
 DevBounds device_bounds(Ctx& c, float t, int mode);
 
@@ -48,6 +49,7 @@ struct JoinState {
     float* osim = nullptr;
     uint64_t n_res = 0;
     uint64_t res_cap_hint = 0;   // exact result count after an overflow
+    uint64_t res_cap_user = 0;   // caller's result capacity (fgss_join_opts.result_capacity)
     uint32_t overflow_retries = 0;
     uint32_t status_host = 0;
     unsigned long long stats_host[SS_N] = {};

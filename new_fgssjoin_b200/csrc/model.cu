@@ -129,9 +129,9 @@ __global__ void k_zero(float* p, int n) {
     for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = 0.f;
 }
 
-// Predicted cost per query and the sum of predicted results (rounded up).
+// Predicted candidates per query and the sum of predicted results (rounded up).
 __global__ void __launch_bounds__(256) k_mlp_predict(const float* __restrict__ feat, uint64_t n,
-                                                     const float* __restrict__ Pg, uint32_t* __restrict__ cost,
+                                                     const float* __restrict__ Pg, uint32_t* __restrict__ pred,
                                                      unsigned long long* res_sum) {
     __shared__ float P[kParamsAll];
     for (int i = threadIdx.x; i < kParamsAll; i += blockDim.x) P[i] = Pg[i];
@@ -143,11 +143,9 @@ __global__ void __launch_bounds__(256) k_mlp_predict(const float* __restrict__ f
 #pragma unroll
         for (int f = 0; f < kFeatM; f++) x[f] = feat[i * kFeatM + f] * kInScale;
         mlp_fwd(P, x, hpre, o);
-        float lw = fminf(fmaxf(o[0] * kOutScale, 0.f), 30.f);
+        float lc = fminf(fmaxf(o[0] * kOutScale, 0.f), 30.f);
         float lr = fminf(fmaxf(o[1] * kOutScale, 0.f), 30.f);
-        float lq = expm1f(feat[i * kFeatM + 0]);
-        float cst = expm1f(lw) + lq;
-        cost[i] = (uint32_t)fminf(cst, 1.0e9f);
+        pred[i] = (uint32_t)fminf(expm1f(lc), 1.0e9f);
         rs += (unsigned long long)ceilf(expm1f(lr) * calib);
     }
     rs = warp_sum(rs);
@@ -169,9 +167,9 @@ void model_sum_cost(Ctx& c, const uint32_t* cost, uint64_t n, uint64_t* out) {
     FGSS_LAUNCH_CK();
 }
 
-void model_predict(Ctx& c, const float* feat, uint64_t n, uint32_t* cost, uint64_t* res_sum) {
+void model_predict(Ctx& c, const float* feat, uint64_t n, uint32_t* pred, uint64_t* res_sum) {
     if (!c.model || !c.model->dev) fail(FGSS_ERR_INVALID, "no cost model loaded");
-    k_mlp_predict<<<grid_for(n, 256, c.num_sms * 8), 256, 0, c.stream>>>(feat, n, c.model->dev, cost,
+    k_mlp_predict<<<grid_for(n, 256, c.num_sms * 8), 256, 0, c.stream>>>(feat, n, c.model->dev, pred,
                                                                         (unsigned long long*)res_sum);
     FGSS_LAUNCH_CK();
 }

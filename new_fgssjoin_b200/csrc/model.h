@@ -1,6 +1,6 @@
 // model.h -- the learned cost model of the batched method: a 2-layer FP32 MLP
 // (kFeat inputs -> kHidden ReLU -> 2 outputs) predicting, per query record,
-// log1p(window entries the filter reads) and log1p(result pairs it emits).
+// log1p(candidates it must verify) and log1p(result pairs it emits).
 // Training and inference are our own CUDA kernels (model.cu).  The model is
 // advisory only: it sizes the result buffers and balances work items; an
 // undersized buffer is detected on the device and the join re-runs exactly.
@@ -32,12 +32,12 @@ struct fgss_model {
 
 namespace fgss {
 
-// cost[q] <- expm1(pred window) + len (u32); *res_sum += sum of predicted results (x calib)
-void model_predict(Ctx& c, const float* feat, uint64_t n, uint32_t* cost, uint64_t* res_sum);
+// pred[q] <- predicted candidates (u32); *res_sum += sum of predicted results (x calib)
+void model_predict(Ctx& c, const float* feat, uint64_t n, uint32_t* pred, uint64_t* res_sum);
 // *out += sum of cost[0..n)
 void model_sum_cost(Ctx& c, const uint32_t* cost, uint64_t n, uint64_t* out);
 // Full-batch Adam training on (feat, target) rows already on the device;
-// target rows are (log1p window, log1p results).  Returns the final loss.
+// target rows are (log1p candidates, log1p results).  Returns the final loss.
 float model_fit(Ctx& c, const float* feat, const float* target, uint64_t n, int epochs, float lr, uint64_t seed);
 // One gradient evaluation (for tests): params (kParams) -> grads (kParams), returns loss.
 float model_grad(Ctx& c, const float* feat, const float* target, uint64_t n, const float* params, float* grads);

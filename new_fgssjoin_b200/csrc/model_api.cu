@@ -25,10 +25,10 @@ __global__ void k_res_hist(const uint32_t* __restrict__ oq, uint64_t R, uint32_t
         atomicAdd(&rcnt[oq[i]], 1u);
 }
 
-__global__ void k_targets(const uint32_t* __restrict__ wcnt, const uint32_t* __restrict__ rcnt, uint64_t n,
+__global__ void k_targets(const uint32_t* __restrict__ vcnt, const uint32_t* __restrict__ rcnt, uint64_t n,
                           float* __restrict__ target) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        target[2 * i] = log1pf((float)wcnt[i]);
+        target[2 * i] = log1pf((float)vcnt[i]);
         target[2 * i + 1] = log1pf((float)rcnt[i]);
     }
 }
@@ -72,7 +72,7 @@ fgss_status fgss_model_train(fgss_ctx* ctx, const fgss_sets_view* sets, const fl
             k_features<<<grid_for(m * 32, 256, c.num_sms * 32), 256, 0, c.stream>>>(J.args, J.t, feat + off * kFeat,
                                                                                    cost);
             FGSS_LAUNCH_CK();
-            k_targets<<<grid_for(m, 256, c.num_sms * 8), 256, 0, c.stream>>>(J.args.wcnt, rcnt, m, target + off * 2);
+            k_targets<<<grid_for(m, 256, c.num_sms * 8), 256, 0, c.stream>>>(J.args.vcnt, rcnt, m, target + off * 2);
             FGSS_LAUNCH_CK();
             off += m;
             res_total += J.n_res;
@@ -97,6 +97,27 @@ fgss_status fgss_model_train(fgss_ctx* ctx, const fgss_sets_view* sets, const fl
         c.sync();
         if (final_loss) *final_loss = loss;
         c.last_error.clear();
+        return FGSS_OK;
+    } catch (const Error& e) {
+        ctx->c.last_error = e.msg;
+        return e.st;
+    }
+}
+
+int fgss_model_num_params(void) { return kParams; }
+
+fgss_status fgss_model_grad(fgss_ctx* ctx, const float* feat, const float* target, uint64_t n, const float* params,
+                            float* grads, float* loss) {
+    if (!ctx || !feat || !target || !params || !grads || n == 0) return FGSS_ERR_INVALID;
+    try {
+        Ctx& c = ctx->c;
+        FGSS_CK(cudaSetDevice(c.device));
+        float* df = c.devT<float>("mg.feat", n * kFeat);
+        float* dt = c.devT<float>("mg.target", n * 2);
+        FGSS_CK(cudaMemcpyAsync(df, feat, n * kFeat * 4, cudaMemcpyHostToDevice, c.stream));
+        FGSS_CK(cudaMemcpyAsync(dt, target, n * 2 * 4, cudaMemcpyHostToDevice, c.stream));
+        float l = model_grad(c, df, dt, n, params, grads);
+        if (loss) *loss = l;
         return FGSS_OK;
     } catch (const Error& e) {
         ctx->c.last_error = e.msg;
