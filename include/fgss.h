@@ -205,6 +205,24 @@ void fgss_pairs_free(fgss_pairs* p);
  * (block.cu:193).  Writes to the FILE* given as a void* (stdout if NULL). */
 fgss_status fgss_pairs_print(const fgss_pairs* p, void* file);
 
+/* ------------------------------------------------------------- autotuner */
+
+typedef struct fgss_tune_result {
+    int threads;       /* CTA size of the fused filter+verify kernel */
+    int hash_log2;     /* shared-memory slot table size (log2) */
+    int ctas_per_sm;   /* resident CTAs per SM (0 = as many as fit) */
+    float ms;          /* best filter+verify time measured (device) */
+    char key[64];      /* workload class the choice is cached under */
+} fgss_tune_result;
+
+/* Times every launch shape of the batched method's fused kernel on this join
+ * (reps runs each, best kept) and caches the fastest for its workload class
+ * (threshold, record-count and average-size buckets), in the context and in
+ * the JSON file of fgss_options.tune_cache_path when one was given.  Later
+ * batched joins of the same class use it.  No reference counterpart. */
+fgss_status fgss_autotune(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_join_opts* opts, int reps,
+                          fgss_tune_result* best);
+
 /* ------------------------------------------------------- learned cost model */
 
 /* Trains the 2-layer FP32 MLP of the batched method on counts logged by the

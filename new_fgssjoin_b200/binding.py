@@ -18,7 +18,7 @@ EXPORTED_SYMBOLS = [
     "fgss_tok_opts_default", "fgss_tokenize",
     "fgss_join_opts_default", "fgss_selfjoin", "fgss_selfjoin_batch", "fgss_pairs_free", "fgss_pairs_print",
     "fgss_model_train", "fgss_model_save", "fgss_model_load", "fgss_model_grad", "fgss_model_num_params",
-    "fgss_bounds_table", "fgss_dev_exclusive_scan_u32", "fgss_dev_sort_pairs_u64",
+    "fgss_autotune", "fgss_bounds_table", "fgss_dev_exclusive_scan_u32", "fgss_dev_sort_pairs_u64",
 ]
 
 _u32p = ctypes.POINTER(ctypes.c_uint32)
@@ -68,6 +68,11 @@ class _Pairs(ctypes.Structure):
                 ("cand", _u32p), ("n_cand", ctypes.c_uint64), ("priv", ctypes.c_void_p)]
 
 
+class _TuneResult(ctypes.Structure):
+    _fields_ = [("threads", ctypes.c_int), ("hash_log2", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
+                ("ms", ctypes.c_float), ("key", ctypes.c_char * 64)]
+
+
 class FgssError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__("%s (status %d)" % (msg, status))
@@ -112,6 +117,7 @@ def load_library():
     L.fgss_dev_exclusive_scan_u32.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64]
     L.fgss_dev_sort_pairs_u64.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                           ctypes.c_int, ctypes.c_int]
+    L.fgss_autotune.argtypes = [ctypes.c_void_p, P(_View), P(_JoinOpts), ctypes.c_int, P(_TuneResult)]
     L.fgss_bounds_table.argtypes = [ctypes.c_float, ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     _lib = L
@@ -247,12 +253,14 @@ def _stats_dict(st):
 class Context:
     """A libfgss context bound to one CUDA device and stream."""
 
-    def __init__(self, device=0, stream=None, verbose=False):
+    def __init__(self, device=0, stream=None, verbose=False, tune_cache_path=None):
         self._L = load_library()
         o = _Options()
         o.device = device
         o.stream = stream
         o.verbose = int(verbose)
+        self._tune_path = os.fsencode(tune_cache_path) if tune_cache_path else None
+        o.tune_cache_path = self._tune_path
         self._ctx = ctypes.c_void_p()
         st = self._L.fgss_create(ctypes.byref(self._ctx), ctypes.byref(o))
         if st != 0:
@@ -343,6 +351,16 @@ class Context:
         rc = self._L.fgss_selfjoin_batch(self._ctx, views, opts, n, outs, sts)
         _check(self._L, self._ctx, rc)
         return [self._collect(outs[i], sts[i], False) for i in range(n)]
+
+    def autotune(self, sets, threshold, reps=2, bounds="reference"):
+        """Times every fused-kernel launch shape on this join; caches the best."""
+        v = sets.view() if isinstance(sets, Sets) else sets
+        o = self._opts(threshold, "batched", bounds, False, False)
+        r = _TuneResult()
+        _check(self._L, self._ctx, self._L.fgss_autotune(self._ctx, ctypes.byref(v), ctypes.byref(o), reps,
+                                                         ctypes.byref(r)))
+        return {"threads": r.threads, "hash_log2": r.hash_log2, "ctas_per_sm": r.ctas_per_sm, "ms": r.ms,
+                "key": r.key.decode()}
 
     # --------------------------------------------------------------- model
     def model_train(self, sets_list, thresholds, epochs=300, lr=0.01, seed=0):

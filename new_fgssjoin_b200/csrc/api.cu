@@ -6,6 +6,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <memory>
 #include <vector>
 
@@ -242,6 +243,7 @@ fgss_status fgss_create(fgss_ctx** out, const fgss_options* opt) {
             c.own_stream = true;
         }
         for (auto& e : c.ev) FGSS_CK(cudaEventCreate(&e));
+        tune_load(c);
     });
     if (st != FGSS_OK) {
         g_err = ctx->c.last_error;
@@ -357,6 +359,59 @@ fgss_status fgss_pairs_print(const fgss_pairs* p, void* file) {
     for (uint64_t i = 0; i < p->n; i++)
         fprintf(f, "%d %d %f\n", (int)p->id_q[i], (int)p->id_s[i], (double)p->sim[i]);  // block.cu:193
     return FGSS_OK;
+}
+
+fgss_status fgss_autotune(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_join_opts* opts, int reps,
+                          fgss_tune_result* best) {
+    if (!ctx || !sets || !opts || reps <= 0) return FGSS_ERR_INVALID;
+    return guard(ctx, [&] {
+        Ctx& c = ctx->c;
+        FGSS_CK(cudaSetDevice(c.device));
+        fgss_join_opts o = *opts;
+        o.method = FGSS_METHOD_BATCHED;
+        o.want_candidates = 0;
+        o.out_on_device = 1;
+        const std::string key = tune_key(sets->n_sets, sets->n_tokens, o.threshold);
+        TuneEntry win;
+        win.ms = 1e30f;
+        for (int i = 0; i < kNumFusedShapes; i++) {
+            TuneEntry te;
+            te.threads = kFusedShapes[i][0];
+            te.hash_log2 = kFusedShapes[i][1];
+            te.ctas_per_sm = 0;
+            c.tune_force = &te;
+            float bestms = 1e30f;
+            for (int r = 0; r < reps; r++) {
+                fgss_pairs p;
+                fgss_stats st;
+                try {
+                    run_joins(c, sets, &o, 1, &p, &st);
+                } catch (...) {
+                    c.tune_force = nullptr;
+                    throw;
+                }
+                fgss_pairs_free(&p);
+                bestms = std::min(bestms, st.ms_filter);
+            }
+            c.tune_force = nullptr;
+            if (c.verbose)
+                fprintf(stderr, "[fgss] autotune %s: threads %d hash_log2 %d -> %.3f ms\n", key.c_str(), te.threads,
+                        te.hash_log2, bestms);
+            if (bestms < win.ms) {
+                win = te;
+                win.ms = bestms;
+            }
+        }
+        c.tune[key] = win;
+        tune_save(c);
+        if (best) {
+            best->threads = win.threads;
+            best->hash_log2 = win.hash_log2;
+            best->ctas_per_sm = win.ctas_per_sm;
+            best->ms = win.ms;
+            snprintf(best->key, sizeof best->key, "%s", key.c_str());
+        }
+    });
 }
 
 fgss_status fgss_bounds_table(float threshold, int bounds, uint32_t max_len, uint16_t* probe, uint16_t* index,

@@ -93,8 +93,8 @@ static void launch_fused(Ctx& c, const JoinArgs* d_args, const FusedArgs* d_farg
 }
 
 // Launch shapes the autotuner chooses from.
-const int kFusedShapes[][2] = {{128, 10}, {128, 11}, {256, 11}, {256, 12}, {512, 12}, {512, 13}};
-const int kNumFusedShapes = 6;
+extern const int kFusedShapes[][2] = {{128, 10}, {128, 11}, {256, 11}, {256, 12}, {512, 12}, {512, 13}};
+extern const int kNumFusedShapes = 6;
 
 void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const FusedArgs* d_fargs, const uint4* items,
                   uint32_t n_items, uint32_t* counter) {
@@ -180,7 +180,8 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
     uint64_t grand = 0;
     for (size_t i = 0; i < nj; i++) grand += htot[i];
     // items: ~16 per resident CTA over the whole batch, split by cost share
-    const TuneEntry te = c.tune.count("fused") ? c.tune["fused"] : TuneEntry{};
+    const TuneEntry te = c.tune_force ? *c.tune_force
+                                      : tune_lookup(c, tune_key(joins[0]->in.n_sets, joins[0]->in.n_tokens, joins[0]->t));
     const uint64_t want = (uint64_t)16 * c.num_sms * std::max(1, te.ctas_per_sm);
     std::vector<uint32_t> K(nj, 0);
     uint64_t nitems = 0;

@@ -40,6 +40,7 @@ struct Ctx {
     std::map<std::string, DevBuf> bufs;
     std::map<std::string, DevBuf> host_bufs;  // pinned
     std::map<std::string, TuneEntry> tune;
+    const TuneEntry* tune_force = nullptr;  // set by the autotuner while it times a shape
     fgss_model* model = nullptr;
     cudaEvent_t ev[8] = {};
     bool probe_timed = false;  // ev[4]..ev[5] bracket the last fused filter+verify launch

@@ -248,54 +248,70 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                 }
             }
         };
+        // The whole warp iterates together until every lane has drained the list;
+        // lanes without a candidate take the next slots with one atomic per warp.
+        bool drained = false;
         for (;;) {
-            if (!have) {
-                const uint32_t i = atomicAdd(&s_next, 1u);
-                if (i >= nocc) break;
-                const unsigned long long v = slots[occ[i]];
-                s = (uint32_t)(v >> 32);
-                c = ((uint32_t)v >> 16) & 0xffffu;
-                const uint32_t jm = (uint32_t)v & 0xffffu;
-                ls = a.len[s];
-                st = a.tok + a.pos[s];
-                const uint4 sm = fa.smin[lq + ls];
-                const uint32_t ips = a.index[ls];
-                xq = qtok[jm];
-                const uint32_t A = lq - jm;
-                const bool cand = (c + A >= sm.x) && smax_le(st, (int)ls + (int)c - (int)sm.x, c, ips, xq);
-                const bool ver = (c + A - 1 >= sm.y) && smax_le(st, (int)ls + (int)c - 1 - (int)sm.y, c, ips, xq);
-                my_cand += cand;
-                if (!ver) continue;
-                im = sm.y;
-                need = sm.z;
-                qrest = lq - jm - 1;
-                cnt = c;
-                k = c;  // the last match sits at or after position c - 1
-                p0 = k;
-                if (k >= ls || cnt + min(ls - k, qrest) < im) {
-                    tally(c, k);
-                    continue;
-                }
-                have = true;
+            const uint32_t want = __ballot_sync(kFull, !have && !drained);
+            uint32_t i = 0xffffffffu;
+            if (want) {
+                const uint32_t leader = __ffs(want) - 1;
+                uint32_t base = 0;
+                if (lane == leader) base = atomicAdd(&s_next, (uint32_t)__popc(want));
+                base = __shfl_sync(kFull, base, leader);
+                i = base + __popc(want & lanemask_lt());
             }
-            // one 16-byte step of the merge
-            const uintptr_t addr = reinterpret_cast<uintptr_t>(st + k);
-            const uint4 v4 = __ldg(reinterpret_cast<const uint4*>(addr & ~uintptr_t(15)));
-            const uint32_t off = (uint32_t)(addr & 15u) >> 2;
-            const uint32_t n_in = min(4u - off, ls - k);
-            const uint32_t xs[4] = {v4.x, v4.y, v4.z, v4.w};
+            if (!have && !drained) {
+                if (i >= nocc) {
+                    drained = true;
+                } else {
+                    const unsigned long long v = slots[occ[i]];
+                    s = (uint32_t)(v >> 32);
+                    c = ((uint32_t)v >> 16) & 0xffffu;
+                    const uint32_t jm = (uint32_t)v & 0xffffu;
+                    ls = a.len[s];
+                    st = a.tok + a.pos[s];
+                    const uint4 sm = fa.smin[lq + ls];
+                    const uint32_t ips = a.index[ls];
+                    xq = qtok[jm];
+                    const uint32_t A = lq - jm;
+                    const bool cand = (c + A >= sm.x) && smax_le(st, (int)ls + (int)c - (int)sm.x, c, ips, xq);
+                    const bool ver =
+                        (c + A - 1 >= sm.y) && smax_le(st, (int)ls + (int)c - 1 - (int)sm.y, c, ips, xq);
+                    my_cand += cand;
+                    if (ver) {
+                        im = sm.y;
+                        need = sm.z;
+                        qrest = lq - jm - 1;
+                        cnt = c;
+                        k = c;  // the last match sits at or after position c - 1
+                        p0 = k;
+                        if (k >= ls || cnt + min(ls - k, qrest) < im) tally(c, k);
+                        else have = true;
+                    }
+                }
+            }
+            if (have) {
+                // one 16-byte step of the merge
+                const uintptr_t addr = reinterpret_cast<uintptr_t>(st + k);
+                const uint4 v4 = __ldg(reinterpret_cast<const uint4*>(addr & ~uintptr_t(15)));
+                const uint32_t off = (uint32_t)(addr & 15u) >> 2;
+                const uint32_t n_in = min(4u - off, ls - k);
+                const uint32_t xs[4] = {v4.x, v4.y, v4.z, v4.w};
 #pragma unroll
-            for (uint32_t t = 0; t < 4; t++) {
-                if (t >= off && t < off + n_in) {
-                    const uint32_t x = xs[t];
-                    if (x > xq && bm_test(bm, exact_bm, x, qtok, 0, lq)) cnt++;
+                for (uint32_t t = 0; t < 4; t++) {
+                    if (t >= off && t < off + n_in) {
+                        const uint32_t x = xs[t];
+                        if (x > xq && bm_test(bm, exact_bm, x, qtok, 0, lq)) cnt++;
+                    }
+                }
+                k += n_in;
+                if (k >= ls || cnt + min(ls - k, qrest - (cnt - c)) < im) {
+                    have = false;
+                    tally(cnt, k);
                 }
             }
-            k += n_in;
-            if (k >= ls || cnt + min(ls - k, qrest - (cnt - c)) < im) {
-                have = false;
-                tally(cnt, k);
-            }
+            if (__all_sync(kFull, drained)) break;
         }
         my_cand = warp_sum(my_cand);
         if (lane == 0 && my_cand) atomicAdd(&s_cand, my_cand);
@@ -316,7 +332,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
 }
 
 template <int NT, int HLOG>
-__global__ void __launch_bounds__(NT) k_fused(const JoinArgs* __restrict__ joins, const FusedArgs* __restrict__ fargs,
+__global__ void __launch_bounds__(NT, 1024 / NT) k_fused(const JoinArgs* __restrict__ joins, const FusedArgs* __restrict__ fargs,
                                               const uint4* __restrict__ items, uint32_t n_items,
                                               uint32_t* item_counter) {
     extern __shared__ __align__(16) unsigned char smem[];

@@ -72,4 +72,13 @@ struct BatchPlan {
 };
 void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_model);
 
+// Autotuner (tune.cu): workload class of a join, the shapes to try, the
+// cache file.
+std::string tune_key(uint64_t n, uint64_t n_tokens, float t);
+extern const int kFusedShapes[][2];
+extern const int kNumFusedShapes;
+TuneEntry tune_lookup(Ctx& c, const std::string& key);
+void tune_load(Ctx& c);
+void tune_save(Ctx& c);
+
 }  // namespace fgss

@@ -199,3 +199,18 @@ def test_kmer_reads_vs_oracle(ctx):
         got = ctx.selfjoin(s, 0.8, method=method)
         ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, 0.8)
         _check_same(got, ref, st)
+
+
+def test_autotuner_picks_a_shape_and_caches_it(tmp_path, titles_sets):
+    path = tmp_path / "tune.json"
+    with F.Context(device=0, tune_cache_path=str(path)) as c2:
+        best = c2.autotune(titles_sets, 0.7, reps=1)
+        assert best["threads"] in (128, 256, 512) and best["ms"] > 0
+        got = c2.selfjoin(titles_sets, 0.7, method="batched")
+    ref, st = O.join(titles_sets.pos, titles_sets.len, titles_sets.tokens, titles_sets.n_terms, 0.7)
+    _check_same(got, ref, st)
+    txt = path.read_text()
+    assert best["key"] in txt
+    with F.Context(device=0, tune_cache_path=str(path)) as c3:  # reloads the cache
+        got = c3.selfjoin(titles_sets, 0.7, method="batched")
+        _check_same(got, ref, st)
