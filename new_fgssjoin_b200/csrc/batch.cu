@@ -93,8 +93,8 @@ static void launch_fused(Ctx& c, const JoinArgs* d_args, const FusedArgs* d_farg
 }
 
 // Launch shapes the autotuner chooses from.
-extern const int kFusedShapes[][2] = {{128, 10}, {128, 11}, {256, 11}, {256, 12}, {512, 12}, {512, 13}};
-extern const int kNumFusedShapes = 6;
+extern const int kFusedShapes[][2] = {{64, 9}, {64, 10}, {128, 9}, {128, 10}, {128, 11}, {256, 11}, {256, 12}};
+extern const int kNumFusedShapes = 7;
 
 void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const FusedArgs* d_fargs, const uint4* items,
                   uint32_t n_items, uint32_t* counter) {
@@ -103,14 +103,15 @@ void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const Fus
         launch_fused<NT, HL>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm); \
         return;                                                                            \
     }
+    FGSS_F(64, 9)
+    FGSS_F(64, 10)
+    FGSS_F(128, 9)
     FGSS_F(128, 10)
     FGSS_F(128, 11)
     FGSS_F(256, 11)
     FGSS_F(256, 12)
-    FGSS_F(512, 12)
-    FGSS_F(512, 13)
 #undef FGSS_F
-    launch_fused<256, 11>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm);
+    launch_fused<128, 10>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm);
 }
 
 // Work-item cost of a query: exact window entries + a verification estimate.
@@ -300,3 +301,14 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
 }
 
 }  // namespace fgss
+
+#ifdef FGSS_PHASE_PROFILE
+// Reads and clears the fused kernel's per-phase cycle counters (profiling builds only).
+extern "C" int fgss_phase_cycles(unsigned long long* out, int n) {
+    if (n > 8) n = 8;
+    if (cudaMemcpyFromSymbol(out, fgss::g_phase_cycles, n * sizeof(unsigned long long)) != cudaSuccess) return -1;
+    unsigned long long z[8] = {};
+    cudaMemcpyToSymbol(fgss::g_phase_cycles, z, sizeof z);
+    return n;
+}
+#endif

@@ -24,6 +24,24 @@
 
 namespace fgss {
 
+// Optional per-phase cycle accounting of the fused kernel (thread 0 of every
+// CTA), compiled in only with -DFGSS_PHASE_PROFILE; no effect otherwise.
+#ifdef FGSS_PHASE_PROFILE
+__device__ unsigned long long g_phase_cycles[8];
+#define FGSS_PHASE_START() long long fgss_pt_ = clock64()
+#define FGSS_PHASE(i)                                                                   \
+    do {                                                                                \
+        if (threadIdx.x == 0) {                                                         \
+            long long n_ = clock64();                                                   \
+            atomicAdd(&g_phase_cycles[i], (unsigned long long)(n_ - fgss_pt_));         \
+            fgss_pt_ = n_;                                                              \
+        }                                                                               \
+    } while (0)
+#else
+#define FGSS_PHASE_START() (void)0
+#define FGSS_PHASE(i) (void)0
+#endif
+
 // Layout: slots u64[H] | occ u16[H] | wlo,whi,clo u32[PC] | wpre u32[PC+4] | qtok u32[QC] | bm u32[BW]
 template <int HLOG>
 struct FusedLayout {
@@ -117,6 +135,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
         return;
     }
     const bool exact_bm = a.n_terms <= Lay::BW * 32;
+    FGSS_PHASE_START();
     const uint32_t* qt = a.tok + a.pos[q];
     const uint2* qwin = fa.win + fa.poff[q];
     for (uint32_t j = tid; j < lq; j += NT) {
@@ -139,6 +158,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     }
     for (;;) {
         __syncthreads();
+        FGSS_PHASE(0);  // staging / previous chunk's clear
         const uint32_t sp = s_sp;
         if (sp == 0) break;
         const uint32_t ra = s_sa[sp - 1], rb = s_sb[sp - 1];
@@ -177,6 +197,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
             }
         }
         __syncthreads();
+        FGSS_PHASE(1);  // chunk windows + scan
         const uint32_t L = s_L;
         if (L > Lay::cap && rb - ra > 1) {
             if (tid == 0) {
@@ -231,6 +252,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
             if (!done) atomicOr(a.status, ST_HASH_FULL);
         }
         __syncthreads();
+        FGSS_PHASE(2);  // accumulate
         // lane-persistent decide + merge over the occupied slots
         const uint32_t nocc = s_nocc;
         uint32_t my_cand = 0;
@@ -316,6 +338,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
         my_cand = warp_sum(my_cand);
         if (lane == 0 && my_cand) atomicAdd(&s_cand, my_cand);
         __syncthreads();
+        FGSS_PHASE(3);  // decide + merge
         for (uint32_t i = tid; i < nocc; i += NT) slots[occ[i]] = kEmptySlot;
     }
     __syncthreads();
