@@ -142,6 +142,9 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
     std::vector<uint32_t*> pre(nj);
     FGSS_CK(cudaMemsetAsync(d_tot, 0, (nj * 2 + 2) * 8, c.stream));
     std::vector<FusedArgs> hf(nj);
+    const TuneEntry te = c.tune_force ? *c.tune_force
+                                      : tune_lookup(c, tune_key(joins[0]->in.n_sets, joins[0]->in.n_tokens, joins[0]->t));
+    const uint32_t cap_entries = (1u << te.hash_log2) / 2;  // chunk capacity of the chosen kernel shape
     for (size_t i = 0; i < nj; i++) {
         JoinState& J = *joins[i];
         const uint64_t n = J.in.n_sets;
@@ -159,8 +162,20 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         if (n == 0) continue;
         // windows of every probe token (exact per-query work), then features and the learned estimate
         exclusive_scan<uint32_t>(c, J.pcnt, poff, n, nullptr, (uint32_t*)nullptr, J.pfx("scan.p").c_str());
-        k_windows<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wtot);
+        uint4* meta = c.devT<uint4>(J.pfx("meta"), n + 1);
+        uint2* qchunk = c.devT<uint2>(J.pfx("qchunk"), n + 1);
+        const uint64_t cbuf_cap = 16 * J.in.n_tokens + 1024;
+        uint32_t* cbuf = c.devT<uint32_t>(J.pfx("cbuf"), cbuf_cap);
+        unsigned long long* cused = reinterpret_cast<unsigned long long*>(J.status + 4);
+        FGSS_CK(cudaMemsetAsync(cused, 0, 8, c.stream));
+        k_windows<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wtot, meta);
         FGSS_LAUNCH_CK();
+        k_chunks<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wtot, cap_entries,
+                                                                            qchunk, cbuf, cbuf_cap, cused);
+        FGSS_LAUNCH_CK();
+        hf[i].meta = meta;
+        hf[i].qchunk = qchunk;
+        hf[i].cbuf = cbuf;
         const bool model = use_model && c.model && !J.res_cap_hint;
         if (model) {
             k_features<<<grid_for(n * 32, 256, c.num_sms * 32), 256, 0, c.stream>>>(J.args, J.t, feat, fcost);
@@ -181,8 +196,6 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
     uint64_t grand = 0;
     for (size_t i = 0; i < nj; i++) grand += htot[i];
     // items: ~16 per resident CTA over the whole batch, split by cost share
-    const TuneEntry te = c.tune_force ? *c.tune_force
-                                      : tune_lookup(c, tune_key(joins[0]->in.n_sets, joins[0]->in.n_tokens, joins[0]->t));
     const uint64_t want = (uint64_t)16 * c.num_sms * std::max(1, te.ctas_per_sm);
     std::vector<uint32_t> K(nj, 0);
     uint64_t nitems = 0;

@@ -63,7 +63,7 @@ struct FusedLayout {
 // Window of every probe token: warp per query.  win[poff[q] + j] = (lo, hi);
 // wtot[q] = sum of the window sizes.
 static __global__ void k_windows(JoinArgs a, const uint32_t* __restrict__ poff, uint2* __restrict__ win,
-                                 uint32_t* __restrict__ wtot) {
+                                 uint32_t* __restrict__ wtot, uint4* __restrict__ meta) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t lane = lane_id();
     const bool unsorted = (*a.status & ST_UNSORTED) != 0;
@@ -86,14 +86,66 @@ static __global__ void k_windows(JoinArgs a, const uint32_t* __restrict__ poff, 
             tot += hi - lo;
         }
         tot = warp_sum(tot);
-        if (lane == 0) wtot[q] = tot;
+        if (lane == 0) {
+            wtot[q] = tot;
+            meta[q] = make_uint4(a.pos[q], lq, lq <= 65535u ? a.index[lq] : 0u, 0u);
+        }
+    }
+}
+
+// Chunk boundaries of the queries whose windows hold more than `cap` entries:
+// the id window [q+1, send) is cut into nch equal id ranges (sized for 3/4 of
+// cap on average) and, for every inner boundary id b and probe token j, the
+// first entry of j's window at or after b is stored.  Warp per query; the
+// boundary buffer is carved with one atomic per query; a query that does not
+// fit keeps nch = 1 and the fused kernel bisects it instead.
+static __global__ void k_chunks(JoinArgs a, const uint32_t* __restrict__ poff, const uint2* __restrict__ win,
+                                const uint32_t* __restrict__ wtot, uint32_t cap, uint2* __restrict__ qchunk,
+                                uint32_t* __restrict__ cbuf, uint64_t cbuf_cap,
+                                unsigned long long* __restrict__ cbuf_used) {
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t lane = lane_id();
+    const bool unsorted = (*a.status & ST_UNSORTED) != 0;
+    for (uint32_t q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < a.n; q += warps) {
+        const uint32_t L = wtot[q];
+        uint32_t nch = 1;
+        unsigned long long base = 0;
+        const uint32_t lq = a.len[q];
+        const uint32_t qp = lq <= 65535u ? a.probe[lq] : 0;
+        const uint32_t send = unsorted ? a.n : (lq <= 65535u ? a.send[lq] : 0);
+        if (L > cap && qp > 0 && send > q + 2) {
+            const uint32_t span = send - q - 1;
+            uint64_t want = ((uint64_t)L * 4 + 3ull * cap - 1) / (3ull * cap);
+            nch = (uint32_t)(want < span ? want : span);
+            if (lane == 0) {
+                const unsigned long long need = (unsigned long long)(nch - 1) * qp;
+                base = atomicAdd(cbuf_used, need);
+                if (base + need > cbuf_cap) nch = 1;
+            }
+            nch = __shfl_sync(kFull, nch, 0);
+            base = __shfl_sync(kFull, base, 0);
+            if (nch > 1) {
+                const uint2* w = win + poff[q];
+                const uint32_t inner = (nch - 1) * qp;
+                for (uint32_t f = lane; f < inner; f += 32) {
+                    const uint32_t i = f / qp + 1, j = f % qp;
+                    const uint32_t b = q + 1 + (uint32_t)(((uint64_t)span * i) / nch);
+                    const uint2 wj = w[j];
+                    cbuf[base + f] = lower_bound_u32(a.ent_s, wj.x, wj.y, b);
+                }
+            }
+        }
+        if (lane == 0) qchunk[q] = make_uint2((uint32_t)base, nch);
     }
 }
 
 struct FusedArgs {
-    const uint32_t* poff;  // per query: first probe window
+    const uint32_t* poff;    // per query: first probe window
     const uint2* win;
-    const uint4* smin;     // per length sum S: (cand_min, inter_min, need, 0)
+    const uint4* smin;       // per length sum S: (cand_min, inter_min, need, 0)
+    const uint4* meta;       // per record: (pos, len, index prefix, 0)
+    const uint2* qchunk;     // per query: (first boundary in cbuf, number of chunks)
+    const uint32_t* cbuf;    // chunk boundaries: per inner boundary, first entry of each probe window
 };
 
 __device__ __forceinline__ bool bm_test(const uint32_t* bm, bool exact, uint32_t x, const uint32_t* qtok, uint32_t qa,
@@ -102,6 +154,34 @@ __device__ __forceinline__ bool bm_test(const uint32_t* bm, bool exact, uint32_t
     bool hit = (bm[b >> 5] >> (b & 31)) & 1u;
     if (hit && !exact) hit = contains_gen(qtok, qa, lq, x);
     return hit;
+}
+
+// One merge step: up to 8 source tokens from position k (two independent
+// 16-byte loads of the aligned chunks holding them; the second only when it
+// holds tokens of this record, so no load leaves the record's 16-byte blocks).
+__device__ __forceinline__ uint32_t merge_step(const uint32_t* __restrict__ st, uint32_t& k, uint32_t ls,
+                                               uint32_t xq, const uint32_t* bm, bool exact, const uint32_t* qt,
+                                               uint32_t lq) {
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(st + k);
+    const uint4* p = reinterpret_cast<const uint4*>(addr & ~uintptr_t(15));
+    const uint32_t off = (uint32_t)(addr & 15u) >> 2;
+    const uint32_t avail = ls - k;  // >= 1
+    const uint4 v0 = __ldg(p);
+    const bool two = avail > 4u - off;
+    uint4 v1 = make_uint4(0, 0, 0, 0);
+    if (two) v1 = __ldg(p + 1);
+    const uint32_t n_in = min(8u - off, avail);
+    const uint32_t xs[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+    uint32_t hits = 0;
+#pragma unroll
+    for (uint32_t t = 0; t < 8; t++) {
+        if (t >= off && t < off + n_in) {
+            const uint32_t x = xs[t];
+            if (x > xq && bm_test(bm, exact, x, qt, 0, lq)) hits++;
+        }
+    }
+    k += n_in;
+    return hits;
 }
 
 template <int NT, int HLOG>
@@ -117,13 +197,14 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     uint32_t* qtok = reinterpret_cast<uint32_t*>(smem + Lay::off_qtok);
     uint32_t* bm = reinterpret_cast<uint32_t*>(smem + Lay::off_bm);
     __shared__ uint32_t s_L, s_sp, s_nocc, s_next, s_cand, s_win;
-    __shared__ uint32_t s_sa[48], s_sb[48];
+    __shared__ uint32_t s_sa[48], s_sb[48], s_sc[48];
     __shared__ uint32_t wsum[33];
 
     const uint32_t tid = threadIdx.x, lane = tid & 31;
     const uint32_t st_bits = *a.status;
     if (st_bits & ST_SKIP_ALL) return;
-    const uint32_t lq = a.len[q];
+    const uint4 qm = fa.meta[q];
+    const uint32_t lq = qm.y;
     if (lq == 0 || lq > 65535u) return;
     const uint32_t qp = a.probe[lq];
     if (qp == 0) return;
@@ -136,8 +217,11 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     }
     const bool exact_bm = a.n_terms <= Lay::BW * 32;
     FGSS_PHASE_START();
-    const uint32_t* qt = a.tok + a.pos[q];
+    const uint32_t* qt = a.tok + qm.x;
     const uint2* qwin = fa.win + fa.poff[q];
+    const uint2 qc = fa.qchunk[q];
+    const uint32_t* cb = fa.cbuf + qc.x;
+    const uint32_t nch = qc.y;
     for (uint32_t j = tid; j < lq; j += NT) {
         const uint32_t x = __ldg(qt + j);
         qtok[j] = x;
@@ -152,194 +236,199 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     if (tid == 0) {
         s_cand = 0;
         s_win = 0;
-        s_sp = 1;
-        s_sa[0] = q + 1;
-        s_sb[0] = send;
+        s_sp = 0;
     }
-    for (;;) {
+    const uint32_t span = send - q - 1;
+    for (uint32_t ci = 0; ci < nch; ci++) {
         __syncthreads();
-        FGSS_PHASE(0);  // staging / previous chunk's clear
-        const uint32_t sp = s_sp;
-        if (sp == 0) break;
-        const uint32_t ra = s_sa[sp - 1], rb = s_sb[sp - 1];
-        {
-            constexpr uint32_t PER = (Lay::PC + NT - 1) / NT;
-            const uint32_t b0 = tid * PER;
-            uint32_t loc[PER];
-            uint32_t sum = 0;
-#pragma unroll
-            for (uint32_t i = 0; i < PER; i++) {
-                const uint32_t j = b0 + i;
-                uint32_t cnt = 0;
-                if (j < qp) {
-                    const uint32_t lo0 = wlo[j], hi0 = whi[j];
-                    const uint32_t lo = (ra == q + 1) ? lo0 : lower_bound_u32(a.ent_s, lo0, hi0, ra);
-                    const uint32_t hi = (rb == send) ? hi0 : lower_bound_u32(a.ent_s, lo, hi0, rb);
-                    cnt = hi - lo;
-                    clo[j] = lo;
-                }
-                loc[i] = cnt;
-                sum += cnt;
-            }
-            uint32_t tot;
-            uint32_t pre = block_excl_scan<uint32_t>(sum, wsum, &tot);
-#pragma unroll
-            for (uint32_t i = 0; i < PER; i++) {
-                const uint32_t j = b0 + i;
-                if (j < qp) wpre[j] = pre;
-                pre += loc[i];
-            }
-            if (tid == 0) {
-                wpre[qp] = tot;
-                s_L = tot;
-                s_nocc = 0;
-                s_next = 0;
-            }
-        }
-        __syncthreads();
-        FGSS_PHASE(1);  // chunk windows + scan
-        const uint32_t L = s_L;
-        if (L > Lay::cap && rb - ra > 1) {
-            if (tid == 0) {
-                const uint32_t mid = ra + (rb - ra) / 2;
-                s_sa[sp - 1] = mid;
-                s_sb[sp - 1] = rb;
-                s_sa[sp] = ra;
-                s_sb[sp] = mid;
-                s_sp = sp + 1;
-            }
-            continue;
-        }
         if (tid == 0) {
-            s_sp = sp - 1;
-            s_win += L;
+            // chunk ci of the precomputed split (tag ci: windows from the boundary buffer)
+            s_sa[0] = q + 1 + (uint32_t)(((uint64_t)span * ci) / nch);
+            s_sb[0] = q + 1 + (uint32_t)(((uint64_t)span * (ci + 1)) / nch);
+            s_sc[0] = ci;
+            s_sp = 1;
         }
-        if (L == 0) continue;
-        int hl = 6;
-        while ((1u << hl) < 2 * L && hl < HLOG) hl++;
-        const uint32_t mask = (1u << hl) - 1;
-        // accumulate; a newly occupied slot goes on the occupied list
-        for (uint32_t f = tid; f < L; f += NT) {
-            const uint32_t j = upper_bound_gen(wpre, 0, qp, f) - 1;
-            const uint32_t k = clo[j] + (f - wpre[j]);
-            const uint32_t s = __ldg(a.ent_s + k);
-            if (unsorted && !size_ok(a, lq, a.len[s])) continue;
-            uint32_t h = hash_slot(s, hl);
-            bool done = false;
-            for (uint32_t it = 0; it <= mask && !done; it++) {
-                unsigned long long old = *(volatile unsigned long long*)&slots[h];
-                for (;;) {
-                    const uint32_t key = (uint32_t)(old >> 32);
-                    unsigned long long nw;
-                    if (key == s) {
-                        const uint32_t lo = (uint32_t)old;
-                        nw = ((unsigned long long)s << 32) | ((((lo >> 16) + 1u) << 16) | max(lo & 0xffffu, j));
-                    } else if (key == kEmpty) {
-                        nw = ((unsigned long long)s << 32) | ((1u << 16) | j);
-                    } else {
-                        break;
-                    }
-                    const unsigned long long prev = atomicCAS(&slots[h], old, nw);
-                    if (prev == old) {
-                        if (key == kEmpty) occ[atomicAdd(&s_nocc, 1u)] = (uint16_t)h;
-                        done = true;
-                        break;
-                    }
-                    old = prev;
-                }
-                if (!done) h = (h + 1) & mask;
-            }
-            if (!done) atomicOr(a.status, ST_HASH_FULL);
-        }
-        __syncthreads();
-        FGSS_PHASE(2);  // accumulate
-        // lane-persistent decide + merge over the occupied slots
-        const uint32_t nocc = s_nocc;
-        uint32_t my_cand = 0;
-        bool have = false;
-        uint32_t s = 0, c = 0, xq = 0, ls = 0, k = 0, cnt = 0, qrest = 0, im = 0, need = 0, p0 = 0;
-        const uint32_t* st = nullptr;
-        auto tally = [&](uint32_t o, uint32_t kend) {
-            ctr.verified++;
-            ctr.merged += kend - p0;
-            if (o >= im && o > 0) {
-                ctr.inter++;
-                if (o >= need) {
-                    ctr.res++;
-                    emit_result(a, q, s, o);
-                }
-            }
-        };
-        // The whole warp iterates together until every lane has drained the list;
-        // lanes without a candidate take the next slots with one atomic per warp.
-        bool drained = false;
         for (;;) {
-            const uint32_t want = __ballot_sync(kFull, !have && !drained);
-            uint32_t i = 0xffffffffu;
-            if (want) {
-                const uint32_t leader = __ffs(want) - 1;
-                uint32_t base = 0;
-                if (lane == leader) base = atomicAdd(&s_next, (uint32_t)__popc(want));
-                base = __shfl_sync(kFull, base, leader);
-                i = base + __popc(want & lanemask_lt());
-            }
-            if (!have && !drained) {
-                if (i >= nocc) {
-                    drained = true;
-                } else {
-                    const unsigned long long v = slots[occ[i]];
-                    s = (uint32_t)(v >> 32);
-                    c = ((uint32_t)v >> 16) & 0xffffu;
-                    const uint32_t jm = (uint32_t)v & 0xffffu;
-                    ls = a.len[s];
-                    st = a.tok + a.pos[s];
-                    const uint4 sm = fa.smin[lq + ls];
-                    const uint32_t ips = a.index[ls];
-                    xq = qtok[jm];
-                    const uint32_t A = lq - jm;
-                    const bool cand = (c + A >= sm.x) && smax_le(st, (int)ls + (int)c - (int)sm.x, c, ips, xq);
-                    const bool ver =
-                        (c + A - 1 >= sm.y) && smax_le(st, (int)ls + (int)c - 1 - (int)sm.y, c, ips, xq);
-                    my_cand += cand;
-                    if (ver) {
-                        im = sm.y;
-                        need = sm.z;
-                        qrest = lq - jm - 1;
-                        cnt = c;
-                        k = c;  // the last match sits at or after position c - 1
-                        p0 = k;
-                        if (k >= ls || cnt + min(ls - k, qrest) < im) tally(c, k);
-                        else have = true;
-                    }
-                }
-            }
-            if (have) {
-                // one 16-byte step of the merge
-                const uintptr_t addr = reinterpret_cast<uintptr_t>(st + k);
-                const uint4 v4 = __ldg(reinterpret_cast<const uint4*>(addr & ~uintptr_t(15)));
-                const uint32_t off = (uint32_t)(addr & 15u) >> 2;
-                const uint32_t n_in = min(4u - off, ls - k);
-                const uint32_t xs[4] = {v4.x, v4.y, v4.z, v4.w};
+            __syncthreads();
+            FGSS_PHASE(0);  // staging / previous chunk's clear
+            const uint32_t sp = s_sp;
+            if (sp == 0) break;
+            const uint32_t ra = s_sa[sp - 1], rb = s_sb[sp - 1], tag = s_sc[sp - 1];
+            {
+                constexpr uint32_t PER = (Lay::PC + NT - 1) / NT;
+                const uint32_t b0 = tid * PER;
+                uint32_t loc[PER];
+                uint32_t sum = 0;
 #pragma unroll
-                for (uint32_t t = 0; t < 4; t++) {
-                    if (t >= off && t < off + n_in) {
-                        const uint32_t x = xs[t];
-                        if (x > xq && bm_test(bm, exact_bm, x, qtok, 0, lq)) cnt++;
+                for (uint32_t i = 0; i < PER; i++) {
+                    const uint32_t j = b0 + i;
+                    uint32_t cnt = 0;
+                    if (j < qp) {
+                        uint32_t lo, hi;
+                        if (tag != 0xffffffffu) {
+                            lo = tag == 0 ? wlo[j] : cb[(tag - 1) * qp + j];
+                            hi = tag + 1 == nch ? whi[j] : cb[tag * qp + j];
+                        } else {
+                            lo = lower_bound_u32(a.ent_s, wlo[j], whi[j], ra);
+                            hi = lower_bound_u32(a.ent_s, lo, whi[j], rb);
+                        }
+                        cnt = hi - lo;
+                        clo[j] = lo;
                     }
+                    loc[i] = cnt;
+                    sum += cnt;
                 }
-                k += n_in;
-                if (k >= ls || cnt + min(ls - k, qrest - (cnt - c)) < im) {
-                    have = false;
-                    tally(cnt, k);
+                uint32_t tot;
+                uint32_t pre = block_excl_scan<uint32_t>(sum, wsum, &tot);
+#pragma unroll
+                for (uint32_t i = 0; i < PER; i++) {
+                    const uint32_t j = b0 + i;
+                    if (j < qp) wpre[j] = pre;
+                    pre += loc[i];
+                }
+                if (tid == 0) {
+                    wpre[qp] = tot;
+                    s_L = tot;
+                    s_nocc = 0;
+                    s_next = 0;
                 }
             }
-            if (__all_sync(kFull, drained)) break;
+            __syncthreads();
+            FGSS_PHASE(1);  // chunk windows + scan
+            const uint32_t L = s_L;
+            if (L > Lay::cap && rb - ra > 1) {
+                if (tid == 0) {  // bisect an oversized range; the lower half first
+                    const uint32_t mid = ra + (rb - ra) / 2;
+                    s_sa[sp - 1] = mid;
+                    s_sb[sp - 1] = rb;
+                    s_sc[sp - 1] = 0xffffffffu;
+                    s_sa[sp] = ra;
+                    s_sb[sp] = mid;
+                    s_sc[sp] = 0xffffffffu;
+                    s_sp = sp + 1;
+                }
+                continue;
+            }
+            if (tid == 0) {
+                s_sp = sp - 1;
+                s_win += L;
+            }
+            if (L == 0) continue;
+            int hl = 6;
+            while ((1u << hl) < 2 * L && hl < HLOG) hl++;
+            const uint32_t mask = (1u << hl) - 1;
+            // accumulate; newly occupied slots go on the occupied list.  A thread's
+            // entries f increase, so its token index j only moves forward.
+            uint32_t j = 0;
+            for (uint32_t f = tid; f < L; f += NT) {
+                while (wpre[j + 1] <= f) j++;
+                const uint32_t k = clo[j] + (f - wpre[j]);
+                const uint32_t s = __ldg(a.ent_s + k);
+                if (unsorted && !size_ok(a, lq, a.len[s])) continue;
+                uint32_t h = hash_slot(s, hl);
+                bool done = false;
+                for (uint32_t it = 0; it <= mask && !done; it++) {
+                    unsigned long long old = *(volatile unsigned long long*)&slots[h];
+                    for (;;) {
+                        const uint32_t key = (uint32_t)(old >> 32);
+                        unsigned long long nw;
+                        if (key == s) {
+                            const uint32_t lo = (uint32_t)old;
+                            nw = ((unsigned long long)s << 32) | ((((lo >> 16) + 1u) << 16) | max(lo & 0xffffu, j));
+                        } else if (key == kEmpty) {
+                            nw = ((unsigned long long)s << 32) | ((1u << 16) | j);
+                        } else {
+                            break;
+                        }
+                        const unsigned long long prev = atomicCAS(&slots[h], old, nw);
+                        if (prev == old) {
+                            if (key == kEmpty) occ[atomicAdd(&s_nocc, 1u)] = (uint16_t)h;
+                            done = true;
+                            break;
+                        }
+                        old = prev;
+                    }
+                    if (!done) h = (h + 1) & mask;
+                }
+                if (!done) atomicOr(a.status, ST_HASH_FULL);
+            }
+            __syncthreads();
+            FGSS_PHASE(2);  // accumulate
+            // lane-persistent decide + merge over the occupied slots; the whole warp
+            // iterates until every lane has drained the list, and lanes without a
+            // candidate take the next slots with one atomic per warp
+            const uint32_t nocc = s_nocc;
+            uint32_t my_cand = 0;
+            bool have = false, drained = false;
+            uint32_t s = 0, c = 0, xq = 0, ls = 0, k = 0, cnt = 0, qrest = 0, im = 0, need = 0, p0 = 0;
+            const uint32_t* st = nullptr;
+            auto tally = [&](uint32_t o, uint32_t kend) {
+                ctr.verified++;
+                ctr.merged += kend - p0;
+                if (o >= im && o > 0) {
+                    ctr.inter++;
+                    if (o >= need) {
+                        ctr.res++;
+                        emit_result(a, q, s, o);
+                    }
+                }
+            };
+            for (;;) {
+                const uint32_t want = __ballot_sync(kFull, !have && !drained);
+                uint32_t i = 0xffffffffu;
+                if (want) {
+                    const uint32_t leader = __ffs(want) - 1;
+                    uint32_t base = 0;
+                    if (lane == leader) base = atomicAdd(&s_next, (uint32_t)__popc(want));
+                    base = __shfl_sync(kFull, base, leader);
+                    i = base + __popc(want & lanemask_lt());
+                }
+                if (!have && !drained) {
+                    if (i >= nocc) {
+                        drained = true;
+                    } else {
+                        const unsigned long long v = slots[occ[i]];
+                        s = (uint32_t)(v >> 32);
+                        c = ((uint32_t)v >> 16) & 0xffffu;
+                        const uint32_t jm = (uint32_t)v & 0xffffu;
+                        const uint4 sm4 = fa.meta[s];  // (pos, len, index prefix)
+                        ls = sm4.y;
+                        st = a.tok + sm4.x;
+                        const uint4 sm = fa.smin[lq + ls];
+                        xq = qtok[jm];
+                        const uint32_t A = lq - jm;
+                        const bool cand =
+                            (c + A >= sm.x) && smax_le(st, (int)ls + (int)c - (int)sm.x, c, sm4.z, xq);
+                        const bool ver =
+                            (c + A - 1 >= sm.y) && smax_le(st, (int)ls + (int)c - 1 - (int)sm.y, c, sm4.z, xq);
+                        my_cand += cand;
+                        if (ver) {
+                            im = sm.y;
+                            need = sm.z;
+                            qrest = lq - jm - 1;
+                            cnt = c;
+                            k = c;  // the last match sits at or after position c - 1
+                            p0 = k;
+                            if (k >= ls || cnt + min(ls - k, qrest) < im) tally(c, k);
+                            else have = true;
+                        }
+                    }
+                }
+                if (have) {
+                    cnt += merge_step(st, k, ls, xq, bm, exact_bm, qtok, lq);
+                    if (k >= ls || cnt + min(ls - k, qrest - (cnt - c)) < im) {
+                        have = false;
+                        tally(cnt, k);
+                    }
+                }
+                if (__all_sync(kFull, drained)) break;
+            }
+            my_cand = warp_sum(my_cand);
+            if (lane == 0 && my_cand) atomicAdd(&s_cand, my_cand);
+            __syncthreads();
+            FGSS_PHASE(3);  // decide + merge
+            for (uint32_t i2 = tid; i2 < nocc; i2 += NT) slots[occ[i2]] = kEmptySlot;
         }
-        my_cand = warp_sum(my_cand);
-        if (lane == 0 && my_cand) atomicAdd(&s_cand, my_cand);
-        __syncthreads();
-        FGSS_PHASE(3);  // decide + merge
-        for (uint32_t i = tid; i < nocc; i += NT) slots[occ[i]] = kEmptySlot;
     }
     __syncthreads();
     if (tid == 0) {

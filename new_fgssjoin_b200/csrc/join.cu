@@ -109,10 +109,10 @@ void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_o
     }
     J.id = J.in.id;
     J.lut = device_bounds(c, J.t, J.bounds);
-    J.status = c.devT<uint32_t>(J.pfx("status"), 4);
+    J.status = c.devT<uint32_t>(J.pfx("status"), 8);
     J.stats = c.devT<unsigned long long>(J.pfx("stats"), SS_N);
     J.maxlen = J.status + 1;
-    FGSS_CK(cudaMemsetAsync(J.status, 0, 16, c.stream));
+    FGSS_CK(cudaMemsetAsync(J.status, 0, 32, c.stream));
     FGSS_CK(cudaMemsetAsync(J.stats, 0, SS_N * 8, c.stream));
     J.icnt = c.devT<uint32_t>(J.pfx("icnt"), n + 1);
     J.pcnt = c.devT<uint32_t>(J.pfx("pcnt"), n + 1);

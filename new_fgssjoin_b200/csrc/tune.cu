@@ -23,8 +23,8 @@ TuneEntry tune_lookup(Ctx& c, const std::string& key) {
     auto it = c.tune.find(key);
     if (it != c.tune.end()) return it->second;
     TuneEntry d;
-    d.threads = 128;
-    d.hash_log2 = 10;
+    d.threads = 64;
+    d.hash_log2 = 9;
     d.ctas_per_sm = 0;
     return d;
 }
