@@ -210,6 +210,7 @@ fgss_status fgss_pairs_print(const fgss_pairs* p, void* file);
 typedef struct fgss_tune_result {
     int threads;       /* CTA size of the fused filter+verify kernel */
     int hash_log2;     /* shared-memory slot table size (log2) */
+    int regs_rt;       /* resident threads per SM the register budget is sized for */
     int ctas_per_sm;   /* resident CTAs per SM (0 = as many as fit) */
     float ms;          /* best filter+verify time measured (device) */
     char key[64];      /* workload class the choice is cached under */

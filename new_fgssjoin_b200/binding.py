@@ -69,7 +69,8 @@ class _Pairs(ctypes.Structure):
 
 
 class _TuneResult(ctypes.Structure):
-    _fields_ = [("threads", ctypes.c_int), ("hash_log2", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
+    _fields_ = [("threads", ctypes.c_int), ("hash_log2", ctypes.c_int), ("regs_rt", ctypes.c_int),
+                ("ctas_per_sm", ctypes.c_int),
                 ("ms", ctypes.c_float), ("key", ctypes.c_char * 64)]
 
 
@@ -359,7 +360,8 @@ class Context:
         r = _TuneResult()
         _check(self._L, self._ctx, self._L.fgss_autotune(self._ctx, ctypes.byref(v), ctypes.byref(o), reps,
                                                          ctypes.byref(r)))
-        return {"threads": r.threads, "hash_log2": r.hash_log2, "ctas_per_sm": r.ctas_per_sm, "ms": r.ms,
+        return {"threads": r.threads, "hash_log2": r.hash_log2, "regs_rt": r.regs_rt, "ctas_per_sm": r.ctas_per_sm,
+                "ms": r.ms,
                 "key": r.key.decode()}
 
     # --------------------------------------------------------------- model

@@ -378,6 +378,7 @@ fgss_status fgss_autotune(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_
             TuneEntry te;
             te.threads = kFusedShapes[i][0];
             te.hash_log2 = kFusedShapes[i][1];
+            te.regs_rt = kFusedShapes[i][2];
             te.ctas_per_sm = 0;
             c.tune_force = &te;
             float bestms = 1e30f;
@@ -395,8 +396,8 @@ fgss_status fgss_autotune(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_
             }
             c.tune_force = nullptr;
             if (c.verbose)
-                fprintf(stderr, "[fgss] autotune %s: threads %d hash_log2 %d -> %.3f ms\n", key.c_str(), te.threads,
-                        te.hash_log2, bestms);
+                fprintf(stderr, "[fgss] autotune %s: threads %d hash_log2 %d regs_rt %d -> %.3f ms\n", key.c_str(),
+                        te.threads, te.hash_log2, te.regs_rt, bestms);
             if (bestms < win.ms) {
                 win = te;
                 win.ms = bestms;
@@ -407,6 +408,7 @@ fgss_status fgss_autotune(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_
         if (best) {
             best->threads = win.threads;
             best->hash_log2 = win.hash_log2;
+            best->regs_rt = win.regs_rt;
             best->ctas_per_sm = win.ctas_per_sm;
             best->ms = win.ms;
             snprintf(best->key, sizeof best->key, "%s", key.c_str());

@@ -74,44 +74,49 @@ __global__ void k_items(const uint32_t* __restrict__ pre, uint32_t n, uint64_t t
     }
 }
 
-template <int NT, int HLOG>
+template <int NT, int HLOG, int RT>
 static void launch_fused(Ctx& c, const JoinArgs* d_args, const FusedArgs* d_fargs, const uint4* items,
                          uint32_t n_items, uint32_t* counter, int ctas_per_sm) {
     static bool attr = false;
     const size_t smem = FusedLayout<HLOG>::bytes;
     if (!attr) {
-        FGSS_CK(cudaFuncSetAttribute(k_fused<NT, HLOG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        FGSS_CK(cudaFuncSetAttribute(k_fused<NT, HLOG, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
     int occ = 0;
-    FGSS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused<NT, HLOG>, NT, smem));
+    FGSS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused<NT, HLOG, RT>, NT, smem));
     if (occ < 1) occ = 1;
     const int per = ctas_per_sm > 0 ? std::min(occ, ctas_per_sm) : occ;
     const unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)per * c.num_sms, std::max<uint32_t>(n_items, 1));
-    k_fused<NT, HLOG><<<grid, NT, smem, c.stream>>>(d_args, d_fargs, items, n_items, counter);
+    k_fused<NT, HLOG, RT><<<grid, NT, smem, c.stream>>>(d_args, d_fargs, items, n_items, counter);
     FGSS_LAUNCH_CK();
 }
 
-// Launch shapes the autotuner chooses from.
-extern const int kFusedShapes[][2] = {{64, 9}, {64, 10}, {128, 9}, {128, 10}, {128, 11}, {256, 11}, {256, 12}};
-extern const int kNumFusedShapes = 7;
+// Launch shapes the autotuner chooses from: CTA size, slot-table log2 size,
+// resident threads per SM the register budget is sized for.
+extern const int kFusedShapes[][3] = {{64, 9, 1024},   {64, 9, 768},    {64, 9, 512},   {64, 10, 1024},
+                                      {128, 9, 1024},  {128, 10, 1024}, {128, 10, 768}, {128, 11, 768},
+                                      {256, 11, 768}};
+extern const int kNumFusedShapes = 9;
 
 void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const FusedArgs* d_fargs, const uint4* items,
                   uint32_t n_items, uint32_t* counter) {
-#define FGSS_F(NT, HL)                                                                     \
-    if (te.threads == NT && te.hash_log2 == HL) {                                          \
-        launch_fused<NT, HL>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm); \
-        return;                                                                            \
+#define FGSS_F(NT, HL, RT)                                                                     \
+    if (te.threads == NT && te.hash_log2 == HL && te.regs_rt == RT) {                          \
+        launch_fused<NT, HL, RT>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm); \
+        return;                                                                                \
     }
-    FGSS_F(64, 9)
-    FGSS_F(64, 10)
-    FGSS_F(128, 9)
-    FGSS_F(128, 10)
-    FGSS_F(128, 11)
-    FGSS_F(256, 11)
-    FGSS_F(256, 12)
+    FGSS_F(64, 9, 1024)
+    FGSS_F(64, 9, 768)
+    FGSS_F(64, 9, 512)
+    FGSS_F(64, 10, 1024)
+    FGSS_F(128, 9, 1024)
+    FGSS_F(128, 10, 1024)
+    FGSS_F(128, 10, 768)
+    FGSS_F(128, 11, 768)
+    FGSS_F(256, 11, 768)
 #undef FGSS_F
-    launch_fused<128, 10>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm);
+    launch_fused<64, 9, 768>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm);
 }
 
 // Work-item cost of a query: exact window entries + a verification estimate.

@@ -22,9 +22,10 @@ struct DevBuf {
 
 // Autotuned launch shapes of the fused filter/verify kernel, per workload class.
 struct TuneEntry {
-    int threads = 256;     // CTA size
-    int hash_log2 = 12;    // shared-memory hash slots (log2)
-    int ctas_per_sm = 2;   // persistent grid = ctas_per_sm x SMs
+    int threads = 64;      // CTA size
+    int hash_log2 = 9;     // shared-memory slot table (log2)
+    int regs_rt = 768;     // resident threads per SM the register budget is sized for
+    int ctas_per_sm = 0;   // persistent grid = ctas_per_sm x SMs (0 = as many as fit)
     float ms = 0.f;        // best time seen
 };
 

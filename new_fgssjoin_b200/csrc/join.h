@@ -75,7 +75,7 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
 // Autotuner (tune.cu): workload class of a join, the shapes to try, the
 // cache file.
 std::string tune_key(uint64_t n, uint64_t n_tokens, float t);
-extern const int kFusedShapes[][2];
+extern const int kFusedShapes[][3];
 extern const int kNumFusedShapes;
 TuneEntry tune_lookup(Ctx& c, const std::string& key);
 void tune_load(Ctx& c);
