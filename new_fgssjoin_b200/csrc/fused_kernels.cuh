@@ -43,7 +43,6 @@ __device__ unsigned long long g_phase_cycles[8];
 #endif
 
 // Layout: slots u64[H] | occ u16[H] | wlo,whi,clo u32[PC] | wpre u32[PC+4] | qtok u32[QC] | bm u32[BW]
-//         | verify list uint4[H/2] (source pos, source, c | last q pos << 16, len | inter_min << 16 ...)
 template <int HLOG>
 struct FusedLayout {
     static constexpr uint32_t H = 1u << HLOG;
@@ -58,8 +57,7 @@ struct FusedLayout {
     static constexpr size_t off_wpre = off_clo + 4ull * PC;
     static constexpr size_t off_qtok = off_wpre + 4ull * (PC + 4);
     static constexpr size_t off_bm = off_qtok + 4ull * QC;
-    static constexpr size_t off_vl = off_bm + 4ull * BW;     // verify list: uint4[cap]
-    static constexpr size_t bytes = off_vl + 16ull * cap;
+    static constexpr size_t bytes = off_bm + 4ull * BW;
 };
 
 // Window of every probe token: warp per query.  win[poff[q] + j] = (lo, hi);
@@ -198,7 +196,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     uint32_t* wpre = reinterpret_cast<uint32_t*>(smem + Lay::off_wpre);
     uint32_t* qtok = reinterpret_cast<uint32_t*>(smem + Lay::off_qtok);
     uint32_t* bm = reinterpret_cast<uint32_t*>(smem + Lay::off_bm);
-    __shared__ uint32_t s_L, s_sp, s_nocc, s_next, s_cand, s_win, s_nv;
+    __shared__ uint32_t s_L, s_sp, s_nocc, s_next, s_cand, s_win;
     __shared__ uint32_t s_sa[48], s_sb[48], s_sc[48];
     __shared__ uint32_t wsum[33];
 
@@ -293,7 +291,6 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                     s_L = tot;
                     s_nocc = 0;
                     s_next = 0;
-                    s_nv = 0;
                 }
             }
             __syncthreads();
@@ -372,67 +369,25 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
             }
             __syncthreads();
             FGSS_PHASE(2);  // accumulate
-            // decide: thread per occupied slot (reference candidate? can a merge still
-            // reach floor(min overlap)?); the ones to merge go on the verify list
+            // lane-persistent decide + merge over the occupied slots; the whole warp
+            // iterates until every lane has drained the list, and lanes without a
+            // candidate take the next slots with one atomic per warp
             const uint32_t nocc = s_nocc;
-            uint4* vlist = reinterpret_cast<uint4*>(smem + Lay::off_vl);
             uint32_t my_cand = 0;
-            for (uint32_t i0 = tid; i0 < nocc; i0 += 2 * NT) {
-                uint4 sm4[2], sm[2];
-                uint32_t sv[2], cv[2], jv[2];
-#pragma unroll
-                for (uint32_t u = 0; u < 2; u++) {
-                    const uint32_t i = i0 + u * NT;
-                    sv[u] = kEmpty;
-                    if (i < nocc) {
-                        const unsigned long long v = slots[occ[i]];
-                        sv[u] = (uint32_t)(v >> 32);
-                        cv[u] = ((uint32_t)v >> 16) & 0xffffu;
-                        jv[u] = (uint32_t)v & 0xffffu;
-                        sm4[u] = fa.meta[sv[u]];  // (pos, len, index prefix)
-                    }
-                }
-#pragma unroll
-                for (uint32_t u = 0; u < 2; u++)
-                    if (sv[u] != kEmpty) sm[u] = fa.smin[lq + sm4[u].y];
-#pragma unroll
-                for (uint32_t u = 0; u < 2; u++) {
-                    if (sv[u] == kEmpty) continue;
-                    const uint32_t c = cv[u], jm = jv[u], ls = sm4[u].y;
-                    const uint32_t* st = a.tok + sm4[u].x;
-                    const uint32_t xq = qtok[jm];
-                    const uint32_t A = lq - jm;
-                    const bool cand = (c + A >= sm[u].x) && smax_le(st, (int)ls + (int)c - (int)sm[u].x, c, sm4[u].z, xq);
-                    const bool ver =
-                        (c + A - 1 >= sm[u].y) && smax_le(st, (int)ls + (int)c - 1 - (int)sm[u].y, c, sm4[u].z, xq);
-                    my_cand += cand;
-                    if (ver) {
-                        const uint32_t qrest = lq - jm - 1;
-                        if (c >= ls || c + min(ls - c, qrest) < sm[u].y) {
-                            // nothing left to merge: c is the overlap
-                            ctr.verified++;
-                            if (c >= sm[u].y && c > 0) {
-                                ctr.inter++;
-                                if (c >= sm[u].z) {
-                                    ctr.res++;
-                                    emit_result(a, q, sv[u], c);
-                                }
-                            }
-                        } else {
-                            const uint32_t vi = atomicAdd(&s_nv, 1u);
-                            vlist[vi] = make_uint4(sm4[u].x, sv[u], c | (jm << 16), ls | (sm[u].y << 16));
-                        }
-                    }
-                }
-            }
-            __syncthreads();
-            // merge: lane-persistent over the verify list; the whole warp iterates
-            // until every lane has drained it, lanes without work take the next
-            // entries with one atomic per warp
-            const uint32_t nv = s_nv;
             bool have = false, drained = false;
-            uint32_t s = 0, c = 0, xq = 0, ls = 0, k = 0, cnt = 0, qrest = 0, im = 0, p0 = 0;
+            uint32_t s = 0, c = 0, xq = 0, ls = 0, k = 0, cnt = 0, qrest = 0, im = 0, need = 0, p0 = 0;
             const uint32_t* st = nullptr;
+            auto tally = [&](uint32_t o, uint32_t kend) {
+                ctr.verified++;
+                ctr.merged += kend - p0;
+                if (o >= im && o > 0) {
+                    ctr.inter++;
+                    if (o >= need) {
+                        ctr.res++;
+                        emit_result(a, q, s, o);
+                    }
+                }
+            };
             for (;;) {
                 const uint32_t want = __ballot_sync(kFull, !have && !drained);
                 uint32_t i = 0xffffffffu;
@@ -444,37 +399,41 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                     i = base + __popc(want & lanemask_lt());
                 }
                 if (!have && !drained) {
-                    if (i >= nv) {
+                    if (i >= nocc) {
                         drained = true;
                     } else {
-                        const uint4 e = vlist[i];
-                        st = a.tok + e.x;
-                        s = e.y;
-                        c = e.z & 0xffffu;
-                        const uint32_t jm = e.z >> 16;
-                        ls = e.w & 0xffffu;
-                        im = e.w >> 16;
+                        const unsigned long long v = slots[occ[i]];
+                        s = (uint32_t)(v >> 32);
+                        c = ((uint32_t)v >> 16) & 0xffffu;
+                        const uint32_t jm = (uint32_t)v & 0xffffu;
+                        const uint4 sm4 = fa.meta[s];  // (pos, len, index prefix)
+                        ls = sm4.y;
+                        st = a.tok + sm4.x;
+                        const uint4 sm = fa.smin[lq + ls];
                         xq = qtok[jm];
-                        qrest = lq - jm - 1;
-                        cnt = c;
-                        k = c;  // the last match sits at or after position c - 1
-                        p0 = k;
-                        have = true;
+                        const uint32_t A = lq - jm;
+                        const bool cand =
+                            (c + A >= sm.x) && smax_le(st, (int)ls + (int)c - (int)sm.x, c, sm4.z, xq);
+                        const bool ver =
+                            (c + A - 1 >= sm.y) && smax_le(st, (int)ls + (int)c - 1 - (int)sm.y, c, sm4.z, xq);
+                        my_cand += cand;
+                        if (ver) {
+                            im = sm.y;
+                            need = sm.z;
+                            qrest = lq - jm - 1;
+                            cnt = c;
+                            k = c;  // the last match sits at or after position c - 1
+                            p0 = k;
+                            if (k >= ls || cnt + min(ls - k, qrest) < im) tally(c, k);
+                            else have = true;
+                        }
                     }
                 }
                 if (have) {
                     cnt += merge_step(st, k, ls, xq, bm, exact_bm, qtok, lq);
                     if (k >= ls || cnt + min(ls - k, qrest - (cnt - c)) < im) {
                         have = false;
-                        ctr.verified++;
-                        ctr.merged += k - p0;
-                        if (cnt >= im && cnt > 0) {
-                            ctr.inter++;
-                            if (cnt >= fa.smin[lq + ls].z) {
-                                ctr.res++;
-                                emit_result(a, q, s, cnt);
-                            }
-                        }
+                        tally(cnt, k);
                     }
                 }
                 if (__all_sync(kFull, drained)) break;

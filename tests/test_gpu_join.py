@@ -205,7 +205,7 @@ def test_autotuner_picks_a_shape_and_caches_it(tmp_path, titles_sets):
     path = tmp_path / "tune.json"
     with F.Context(device=0, tune_cache_path=str(path)) as c2:
         best = c2.autotune(titles_sets, 0.7, reps=1)
-        assert best["threads"] in (128, 256, 512) and best["ms"] > 0
+        assert best["threads"] in (64, 128, 256, 512) and best["ms"] > 0
         got = c2.selfjoin(titles_sets, 0.7, method="batched")
     ref, st = O.join(titles_sets.pos, titles_sets.len, titles_sets.tokens, titles_sets.n_terms, 0.7)
     _check_same(got, ref, st)
