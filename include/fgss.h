@@ -258,6 +258,25 @@ fgss_status fgss_bounds_table(float threshold, int bounds, uint32_t max_len, uin
  * Replaces exclusive_scan<unsigned int> (include/fgssjoin/scan.cuh:39-105). */
 fgss_status fgss_dev_exclusive_scan_u32(fgss_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t n);
 
+/* Exclusive prefix sum of n uint32 values that allocates no device memory,
+ * for callers that cannot call cudaMalloc: a host that pre-allocates all
+ * device memory up front and forbids later allocations, or a latency-critical
+ * loop where cudaMalloc / cudaFree (which synchronizes the device) would
+ * stall it.  No reference counterpart: the reference's scan
+ * (include/fgssjoin/scan.cuh:39-105) allocates through Thrust.
+ *   - Needs no context: it runs on `stream` (a cudaStream_t, NULL = the
+ *     default stream) of the current device and returns once the work is
+ *     queued; the result is ready when the stream reaches that point.
+ *   - Scratch is a fixed 256 KiB array in the library (one per device, kept
+ *     until the process exits), so n is limited to 268,435,456 elements;
+ *     larger n returns FGSS_ERR_CAPACITY (message in fgss_last_error(NULL)).
+ *   - The first call on a device looks the array's device address up once
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - Every call shares that one array: calls that overlap on the GPU (other
+ *     streams, other host threads) race and must be serialized by the caller.
+ * Same result as fgss_dev_exclusive_scan_u32 (out may alias in). */
+fgss_status fgss_dev_exclusive_scan_u32_noalloc(const uint32_t* in, uint32_t* out, uint64_t n, void* stream);
+
 /* Stable LSD radix sort of n (key, value) pairs by key bits [begin_bit, end_bit).
  * No reference counterpart (the reference sorts on the host, preprocess_cli.cpp:170-215). */
 fgss_status fgss_dev_sort_pairs_u64(fgss_ctx* ctx, uint64_t* keys, uint32_t* values, uint64_t n,

@@ -19,6 +19,7 @@ EXPORTED_SYMBOLS = [
     "fgss_join_opts_default", "fgss_selfjoin", "fgss_selfjoin_batch", "fgss_pairs_free", "fgss_pairs_print",
     "fgss_model_train", "fgss_model_save", "fgss_model_load", "fgss_model_grad", "fgss_model_num_params",
     "fgss_autotune", "fgss_bounds_table", "fgss_dev_exclusive_scan_u32", "fgss_dev_sort_pairs_u64",
+    "fgss_dev_exclusive_scan_u32_noalloc",
 ]
 
 _u32p = ctypes.POINTER(ctypes.c_uint32)
@@ -118,6 +119,8 @@ def load_library():
     L.fgss_dev_exclusive_scan_u32.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64]
     L.fgss_dev_sort_pairs_u64.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                           ctypes.c_int, ctypes.c_int]
+    L.fgss_dev_exclusive_scan_u32_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                                      ctypes.c_void_p]
     L.fgss_autotune.argtypes = [ctypes.c_void_p, P(_View), P(_JoinOpts), ctypes.c_int, P(_TuneResult)]
     L.fgss_bounds_table.argtypes = [ctypes.c_float, ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]

@@ -18,8 +18,15 @@
 using namespace fgss;
 
 namespace {
-
 thread_local std::string g_err;
+}
+
+namespace fgss {
+// Message for fgss_last_error(NULL) from entry points that take no context.
+void set_thread_error(const std::string& msg) { g_err = msg; }
+}  // namespace fgss
+
+namespace {
 
 template <typename F>
 fgss_status guard(fgss_ctx* ctx, F&& f) {

@@ -13,7 +13,8 @@ def test_exclusive_scan(ctx, n):
     d_in = torch.from_numpy(a.view(np.int32)).cuda()
     d_out = torch.empty_like(d_in)
     ctx.dev_exclusive_scan_u32(d_in.data_ptr(), d_out.data_ptr(), n)
-    want = np.concatenate([[0], np.cumsum(a.astype(np.uint64))[:-1]]).astype(np.uint32)
+    incl = np.cumsum(a.astype(np.uint64))
+    want = ((incl - a.astype(np.uint64)) & np.uint64(0xFFFFFFFF)).astype(np.uint32)
     assert np.array_equal(d_out.cpu().numpy().view(np.uint32), want)
 
 
