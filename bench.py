@@ -29,6 +29,7 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     "titles100k": dict(kind="titles", n=100_000, seed=2, thresholds=[0.5, 0.6, 0.7, 0.8, 0.9]),
     "heavy1m": dict(kind="heavy", n=1_000_000, seed=3, thresholds=[0.7]),
+    "titles18k": dict(kind="titles", n=18_000, seed=1, thresholds=[0.9]),
 }
 
 

@@ -47,8 +47,8 @@ template <int HLOG>
 struct FusedLayout {
     static constexpr uint32_t H = 1u << HLOG;
     static constexpr uint32_t cap = H / 2;    // window entries per chunk
-    static constexpr uint32_t PC = H / 4;     // probe tokens handled in shared memory
-    static constexpr uint32_t QC = H / 2;     // query tokens staged in shared memory
+    static constexpr uint32_t PC = H / 4 > 256 ? H / 4 : 256;  // probe tokens handled in shared memory
+    static constexpr uint32_t QC = H / 2;     // query tokens staged in shared memory (longer: read from HBM)
     static constexpr uint32_t BW = 1024;      // bitmap words: 32768 bits
     static constexpr size_t off_occ = 8ull * H;
     static constexpr size_t off_wlo = off_occ + 2ull * H;
@@ -211,20 +211,22 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     const bool unsorted = (st_bits & ST_UNSORTED) != 0;
     const uint32_t send = unsorted ? a.n : a.send[lq];
     if (send <= q + 1) return;
-    if (qp > Lay::PC || lq > Lay::QC) {
+    if (qp > Lay::PC) {
         if (tid == 0) defer_heavy(a, q);
         return;
     }
     const bool exact_bm = a.n_terms <= Lay::BW * 32;
     FGSS_PHASE_START();
     const uint32_t* qt = a.tok + qm.x;
+    const bool staged = lq <= Lay::QC;
+    const uint32_t* qsrc = staged ? qtok : qt;  // query tokens: shared memory, or HBM for long records
     const uint2* qwin = fa.win + fa.poff[q];
     const uint2 qc = fa.qchunk[q];
     const uint32_t* cb = fa.cbuf + qc.x;
     const uint32_t nch = qc.y;
     for (uint32_t j = tid; j < lq; j += NT) {
         const uint32_t x = __ldg(qt + j);
-        qtok[j] = x;
+        if (staged) qtok[j] = x;
         const uint32_t b = exact_bm ? x : ((x * 0x9E3779B1u) >> 17);
         atomicOr(&bm[b >> 5], 1u << (b & 31));
     }
@@ -410,7 +412,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                         ls = sm4.y;
                         st = a.tok + sm4.x;
                         const uint4 sm = fa.smin[lq + ls];
-                        xq = qtok[jm];
+                        xq = qsrc[jm];
                         const uint32_t A = lq - jm;
                         const bool cand =
                             (c + A >= sm.x) && smax_le(st, (int)ls + (int)c - (int)sm.x, c, sm4.z, xq);
@@ -430,7 +432,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                     }
                 }
                 if (have) {
-                    cnt += merge_step(st, k, ls, xq, bm, exact_bm, qtok, lq);
+                    cnt += merge_step(st, k, ls, xq, bm, exact_bm, qsrc, lq);
                     if (k >= ls || cnt + min(ls - k, qrest - (cnt - c)) < im) {
                         have = false;
                         tally(cnt, k);
@@ -451,7 +453,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
         ctr.window += s_win;
     }
     for (uint32_t j = tid; j < lq; j += NT) {
-        const uint32_t x = qtok[j];
+        const uint32_t x = qsrc[j];
         const uint32_t b = exact_bm ? x : ((x * 0x9E3779B1u) >> 17);
         bm[b >> 5] = 0u;
     }
