@@ -151,6 +151,7 @@ def main():
     ap.add_argument("--workload", default="titles100k", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-model", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -192,6 +193,12 @@ def main():
         train_text = make_text(w, seed_offset=7919 + rank, n=min(w["n"], 30000))
         train_sets = ctx.tokenize(train_text, **tok_opts(w))
         model_loss = ctx.model_train([train_sets] * len(ts), ts, epochs=300, lr=0.01, seed=1)
+
+    # autotuner (untimed): fastest fused-kernel shape per threshold, cached in the context
+    tuned = {}
+    if not args.no_tune:
+        for t in ts:
+            tuned[str(t)] = ctx.autotune(dev_view(), t, reps=1)
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
 
@@ -274,6 +281,7 @@ def main():
             "speedup_vs_plain": (plain_ms / plain_steps) / per_step,
             "pair_sets_identical": bool(same),
             "candidates_per_step": cands, "results_per_step": R,
+            "autotune": {t: "%dx%d/rt%d" % (v["threads"], v["hash_log2"], v["regs_rt"]) for t, v in tuned.items()},
             "model": {"used": use_model, "train_loss": model_loss,
                       "overflow_retries": sum(s["overflow_retries"] for s in last)},
             "e2e": {"value": ws * cands / (e2e_ms / args.steps * 1e-3), "unit": "candidates/s",

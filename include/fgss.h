@@ -148,6 +148,8 @@ typedef struct fgss_join_opts {
     int use_model;          /* batched method: presize and bin with the learned model */
     uint64_t result_capacity; /* batched method: presized result slots; 0 = learned / automatic.
                                  Too small a value only costs an exact re-run. */
+    uint64_t query_begin;   /* only queries (first records of pairs) in [query_begin, query_end) */
+    uint64_t query_end;     /* are processed; 0, 0 = all.  Used to shard one join over GPUs. */
 } fgss_join_opts;
 
 void fgss_join_opts_default(fgss_join_opts* o);

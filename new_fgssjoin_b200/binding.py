@@ -50,7 +50,8 @@ class _TokOpts(ctypes.Structure):
 class _JoinOpts(ctypes.Structure):
     _fields_ = [("threshold", ctypes.c_float), ("bounds", ctypes.c_int), ("method", ctypes.c_int),
                 ("out_on_device", ctypes.c_int), ("want_candidates", ctypes.c_int), ("use_model", ctypes.c_int),
-                ("result_capacity", ctypes.c_uint64)]
+                ("result_capacity", ctypes.c_uint64), ("query_begin", ctypes.c_uint64),
+                ("query_end", ctypes.c_uint64)]
 
 
 class _Stats(ctypes.Structure):
@@ -307,7 +308,8 @@ class Context:
 
     # ----------------------------------------------------------------- join
     @staticmethod
-    def _opts(threshold, method, bounds, want_candidates, use_model, out_on_device=False, result_capacity=0):
+    def _opts(threshold, method, bounds, want_candidates, use_model, out_on_device=False, result_capacity=0,
+              query_range=None):
         o = _JoinOpts()
         o.threshold = float(threshold)
         o.method = {"plain": METHOD_PLAIN, "batched": METHOD_BATCHED}.get(method, method)
@@ -316,6 +318,8 @@ class Context:
         o.use_model = int(use_model)
         o.out_on_device = int(out_on_device)
         o.result_capacity = int(result_capacity)
+        if query_range is not None:
+            o.query_begin, o.query_end = int(query_range[0]), int(query_range[1])
         return o
 
     def _collect(self, p, st, want_candidates):
@@ -335,10 +339,14 @@ class Context:
         return out
 
     def selfjoin(self, sets, threshold, method="plain", bounds="reference", want_candidates=False,
-                 use_model=False, result_capacity=0):
-        """Self-join of ``sets`` (host Sets or a device view) at ``threshold``."""
+                 use_model=False, result_capacity=0, query_range=None):
+        """Self-join of ``sets`` (host Sets or a device view) at ``threshold``.
+
+        ``query_range`` = (begin, end) processes only the pairs whose first
+        record (memory index) lies in [begin, end): one shard of the join."""
         v = sets.view() if isinstance(sets, Sets) else sets
-        o = self._opts(threshold, method, bounds, want_candidates, use_model, result_capacity=result_capacity)
+        o = self._opts(threshold, method, bounds, want_candidates, use_model, result_capacity=result_capacity,
+                       query_range=query_range)
         p = _Pairs()
         st = _Stats()
         rc = self._L.fgss_selfjoin(self._ctx, ctypes.byref(v), ctypes.byref(o), ctypes.byref(p), ctypes.byref(st))

@@ -55,7 +55,7 @@ __global__ void k_features(JoinArgs a, float t, float* __restrict__ feat, uint32
 
 // Work items of one join: item k = queries with exclusive cost prefix in
 // [k*target, (k+1)*target).
-__global__ void k_items(const uint32_t* __restrict__ pre, uint32_t n, uint64_t total, uint32_t K, uint32_t join,
+__global__ void k_items(const uint64_t* __restrict__ pre, uint32_t n, uint64_t total, uint32_t K, uint32_t join,
                         uint4* __restrict__ items) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
         uint64_t target = (total + K - 1) / K;
@@ -63,7 +63,7 @@ __global__ void k_items(const uint32_t* __restrict__ pre, uint32_t n, uint64_t t
             uint32_t lo = 0, hi = n;
             while (lo < hi) {
                 uint32_t mid = (lo + hi) >> 1;
-                if ((uint64_t)pre[mid] < x) lo = mid + 1;
+                if (pre[mid] < x) lo = mid + 1;
                 else hi = mid;
             }
             return lo;
@@ -121,11 +121,16 @@ void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const Fus
 
 // Work-item cost of a query: exact window entries + a verification estimate.
 __global__ void k_cost(const uint32_t* __restrict__ wtot, const uint32_t* __restrict__ len,
-                       const uint32_t* __restrict__ pred_cand, uint32_t n, uint32_t* __restrict__ cost) {
+                       const uint32_t* __restrict__ pred_cand, uint32_t n, uint32_t q_lo, uint32_t q_hi,
+                       uint64_t* __restrict__ cost) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        if (q < q_lo || q >= q_hi) {  // outside this shard: no work
+            cost[q] = 0;
+            continue;
+        }
         unsigned long long v = (unsigned long long)wtot[q] + len[q];
         if (pred_cand) v += 4ull * pred_cand[q];
-        cost[q] = (uint32_t)min(v, 0x3fffffffull);
+        cost[q] = v;
     }
 }
 
@@ -144,7 +149,7 @@ __global__ void k_clear_filter_state(uint32_t* status, unsigned long long* stats
 void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_model) {
     const size_t nj = joins.size();
     uint64_t* d_tot = c.devT<uint64_t>("b.tot", nj * 2 + 2);
-    std::vector<uint32_t*> pre(nj);
+    std::vector<uint64_t*> pre(nj);
     FGSS_CK(cudaMemsetAsync(d_tot, 0, (nj * 2 + 2) * 8, c.stream));
     std::vector<FusedArgs> hf(nj);
     const TuneEntry te = c.tune_force ? *c.tune_force
@@ -154,13 +159,13 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         JoinState& J = *joins[i];
         const uint64_t n = J.in.n_sets;
         float* feat = c.devT<float>(J.pfx("feat"), (n + 1) * kFeat);
-        uint32_t* cost = c.devT<uint32_t>(J.pfx("cost"), n + 1);
+        uint64_t* cost = c.devT<uint64_t>(J.pfx("cost"), n + 1);
         uint32_t* fcost = c.devT<uint32_t>(J.pfx("fcost"), n + 1);
         uint32_t* poff = c.devT<uint32_t>(J.pfx("poff"), n + 1);
         uint2* win = c.devT<uint2>(J.pfx("win"), J.in.n_tokens + 1);
         uint32_t* wtot = c.devT<uint32_t>(J.pfx("wtot"), n + 1);
         uint32_t* pred = c.devT<uint32_t>(J.pfx("pred"), n + 1);
-        pre[i] = c.devT<uint32_t>(J.pfx("cpre"), n + 1);
+        pre[i] = c.devT<uint64_t>(J.pfx("cpre"), n + 1);
         hf[i].poff = poff;
         hf[i].win = win;
         hf[i].smin = J.lut.smin;
@@ -169,7 +174,7 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         exclusive_scan<uint32_t>(c, J.pcnt, poff, n, nullptr, (uint32_t*)nullptr, J.pfx("scan.p").c_str());
         uint4* meta = c.devT<uint4>(J.pfx("meta"), n + 1);
         uint2* qchunk = c.devT<uint2>(J.pfx("qchunk"), n + 1);
-        const uint64_t cbuf_cap = 16 * J.in.n_tokens + 1024;
+        const uint64_t cbuf_cap = 2 * J.in.n_tokens + (1u << 20);  // overflowing queries bisect instead
         uint32_t* cbuf = c.devT<uint32_t>(J.pfx("cbuf"), cbuf_cap);
         unsigned long long* cused = reinterpret_cast<unsigned long long*>(J.status + 4);
         FGSS_CK(cudaMemsetAsync(cused, 0, 8, c.stream));
@@ -188,10 +193,9 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
             model_predict(c, feat, n, pred, &d_tot[nj + i]);
         }
         k_cost<<<grid_for(n, 256, c.num_sms * 8), 256, 0, c.stream>>>(wtot, J.in.len, model ? pred : nullptr,
-                                                                       (uint32_t)n, cost);
+                                                                       (uint32_t)n, J.args.q_lo, J.args.q_hi, cost);
         FGSS_LAUNCH_CK();
-        exclusive_scan<uint32_t>(c, cost, pre[i], n, nullptr, (uint32_t*)nullptr, J.pfx("scan.cost").c_str());
-        model_sum_cost(c, cost, n, &d_tot[i]);
+        exclusive_scan<uint64_t>(c, cost, pre[i], n, nullptr, &d_tot[i], J.pfx("scan.cost").c_str());
     }
     FusedArgs* d_fargs = c.devT<FusedArgs>("b.fargs", nj);
     FGSS_CK(cudaMemcpyAsync(d_fargs, hf.data(), nj * sizeof(FusedArgs), cudaMemcpyHostToDevice, c.stream));
@@ -217,7 +221,6 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
     for (size_t i = 0; i < nj; i++) {
         if (!K[i]) continue;
         JoinState& J = *joins[i];
-        if (htot[i] >= (1ull << 32)) fail(FGSS_ERR_UNSUPPORTED, "cost prefix exceeds 32 bits");
         k_items<<<grid_for(K[i], 128), 128, 0, c.stream>>>(pre[i], (uint32_t)J.in.n_sets, htot[i], K[i],
                                                             (uint32_t)i, items + off);
         FGSS_LAUNCH_CK();

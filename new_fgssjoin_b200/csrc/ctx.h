@@ -24,7 +24,7 @@ struct DevBuf {
 struct TuneEntry {
     int threads = 64;      // CTA size
     int hash_log2 = 9;     // shared-memory slot table (log2)
-    int regs_rt = 768;     // resident threads per SM the register budget is sized for
+    int regs_rt = 1024;    // resident threads per SM the register budget is sized for
     int ctas_per_sm = 0;   // persistent grid = ctas_per_sm x SMs (0 = as many as fit)
     float ms = 0.f;        // best time seen
 };

@@ -69,7 +69,8 @@ static __global__ void k_windows(JoinArgs a, const uint32_t* __restrict__ poff, 
     const bool unsorted = (*a.status & ST_UNSORTED) != 0;
     for (uint32_t q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < a.n; q += warps) {
         const uint32_t lq = a.len[q];
-        const uint32_t qp = lq <= 65535u ? a.probe[lq] : 0;
+        const bool mine = q >= a.q_lo && q < a.q_hi;
+        const uint32_t qp = (lq <= 65535u && mine) ? a.probe[lq] : 0;
         const uint32_t send = unsorted ? a.n : (lq <= 65535u ? a.send[lq] : 0);
         const uint32_t* qt = a.tok + a.pos[q];
         const uint32_t o = poff[q];
@@ -203,6 +204,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     const uint32_t tid = threadIdx.x, lane = tid & 31;
     const uint32_t st_bits = *a.status;
     if (st_bits & ST_SKIP_ALL) return;
+    if (q < a.q_lo || q >= a.q_hi) return;
     const uint4 qm = fa.meta[q];
     const uint32_t lq = qm.y;
     if (lq == 0 || lq > 65535u) return;

@@ -141,6 +141,14 @@ void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_o
     a.heavy_count = J.status + 2;
     a.heavy_cap = (uint32_t)n;
     a.join_id = (uint32_t)slot;
+    if (o.query_end > o.query_begin) {
+        if (o.query_end > n) fail(FGSS_ERR_INVALID, "query_end beyond the number of records");
+        a.q_lo = (uint32_t)o.query_begin;
+        a.q_hi = (uint32_t)o.query_end;
+    } else {
+        a.q_lo = 0;
+        a.q_hi = (uint32_t)n;
+    }
     J.term_bits = bits_for((uint64_t)v.n_terms + 1);
     if (n == 0) return;
     k_prep<<<grid_for(n, 256, c.num_sms * 16), 256, 0, c.stream>>>(a, J.icnt, J.pcnt, J.maxlen, 1);

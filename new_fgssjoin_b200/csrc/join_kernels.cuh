@@ -94,6 +94,8 @@ struct JoinArgs {
     uint32_t* heavy_count;
     uint32_t heavy_cap;
     uint32_t join_id;
+    uint32_t q_lo;             // queries processed: [q_lo, q_hi) (a shard of the join)
+    uint32_t q_hi;
     uint32_t pad_;
 };
 
@@ -478,6 +480,7 @@ __device__ void probe_query_smem(const JoinArgs& a, uint32_t q, unsigned char* s
     const uint32_t tid = threadIdx.x, lane = tid & 31;
     const uint32_t st_bits = *a.status;
     if (st_bits & ST_SKIP_ALL) return;
+    if (q < a.q_lo || q >= a.q_hi) return;
     const uint32_t lq = a.len[q];
     if (lq == 0 || lq > 65535u) return;
     const uint32_t qp = a.probe[lq];

@@ -25,7 +25,7 @@ TuneEntry tune_lookup(Ctx& c, const std::string& key) {
     TuneEntry d;
     d.threads = 64;
     d.hash_log2 = 9;
-    d.regs_rt = 768;
+    d.regs_rt = 1024;
     d.ctas_per_sm = 0;
     return d;
 }

@@ -323,6 +323,8 @@ static void pv_push(pairvec* v, orc_pair x)
  *   pos/len/tokens: the reference's sets_t arrays; tokens ascending per record.
  *   block_size: the reference's tile edge (block.cu:14-54); 0 means one tile
  *               covering every record.
+ *   q_lo, q_hi: only queries (first records of pairs) in [q_lo, q_hi); 0, 0 = all
+ *               (a shard of the join, for the multi-GPU tests).
  *   want_cands: if nonzero, *cands receives every candidate as
  *               (q, s, partial score) triples -- the cells with score > 0
  *               after filtering (filtering.cu:52-57 / compaction.cu:8-17).
@@ -330,7 +332,8 @@ static void pv_push(pairvec* v, orc_pair x)
  */
 int64_t orc_join(const uint32_t* pos, const uint32_t* len, const uint32_t* tokens,
                  uint32_t n, uint32_t n_terms, float t, uint32_t block_size, int nthreads,
-                 orc_pair** out, orc_stats* st, int want_cands, uint32_t** cands, uint64_t* n_cands)
+                 orc_pair** out, orc_stats* st, int want_cands, uint32_t** cands, uint64_t* n_cands,
+                 uint32_t q_lo, uint32_t q_hi)
 {
     if (!(t > 0.0f && t < 1.0f)) return -ORC_ERR_ARG;
     memset(st, 0, sizeof(*st));
@@ -377,8 +380,10 @@ int64_t orc_join(const uint32_t* pos, const uint32_t* len, const uint32_t* token
         uint32_t* touched = (uint32_t*)malloc(block_size * sizeof(uint32_t));
         pairvec lres = {0, 0, 0};
         pairvec lcv = {0, 0, 0};
+        const int64_t qa = (q_hi > q_lo) ? (int64_t)q_lo : 0;
+        const int64_t qb = (q_hi > q_lo) ? (int64_t)(q_hi < n ? q_hi : n) : (int64_t)n;
 #pragma omp for schedule(dynamic, 16)
-        for (int64_t qq = 0; qq < (int64_t)n; qq++) {
+        for (int64_t qq = qa; qq < qb; qq++) {
             uint32_t query = (uint32_t)qq;
             uint32_t jb = query / block_size;          /* query block */
             uint32_t q_offset = jb * block_size;

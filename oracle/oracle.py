@@ -50,7 +50,7 @@ def lib():
         L.orc_tokenize.restype = ctypes.c_int
         L.orc_join.argtypes = [u32p, u32p, u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
                                ctypes.c_uint32, ctypes.c_int, P(P(_Pair)), P(_Stats), ctypes.c_int,
-                               P(u32p), P(ctypes.c_uint64)]
+                               P(u32p), P(ctypes.c_uint64), ctypes.c_uint32, ctypes.c_uint32]
         L.orc_join.restype = ctypes.c_int64
         L.orc_brute.argtypes = [u32p, u32p, u32p, ctypes.c_uint32, ctypes.c_float, P(P(_Pair))]
         L.orc_brute.restype = ctypes.c_int64
@@ -151,7 +151,7 @@ def encode_bin(ids, lens, tokens):
     return np.concatenate(out).tobytes() if out else b""
 
 
-def join(pos, lens, tokens, n_terms, t, block_size=0, threads=0, want_candidates=False):
+def join(pos, lens, tokens, n_terms, t, block_size=0, threads=0, want_candidates=False, query_range=None):
     """Reference-semantics self-join on MEMORY-order records.
 
     Returns (pairs, stats[, candidates]) where pairs is a structured array
@@ -168,9 +168,10 @@ def join(pos, lens, tokens, n_terms, t, block_size=0, threads=0, want_candidates
     cptr = ctypes.POINTER(ctypes.c_uint32)()
     ncand = ctypes.c_uint64()
     nthreads = threads if threads > 0 else L.orc_num_threads()
+    qb, qe = query_range if query_range else (0, 0)
     n = L.orc_join(pp, lp, tp, len(len_a), int(n_terms), ctypes.c_float(t), block_size, nthreads,
                    ctypes.byref(out), ctypes.byref(st), int(want_candidates), ctypes.byref(cptr),
-                   ctypes.byref(ncand))
+                   ctypes.byref(ncand), int(qb), int(qe))
     if n < 0:
         raise ValueError("orc_join failed: %d" % n)
     pairs = _pairs(out, n)

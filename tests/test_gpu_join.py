@@ -214,3 +214,16 @@ def test_autotuner_picks_a_shape_and_caches_it(tmp_path, titles_sets):
     with F.Context(device=0, tune_cache_path=str(path)) as c3:  # reloads the cache
         got = c3.selfjoin(titles_sets, 0.7, method="batched")
         _check_same(got, ref, st)
+
+
+@pytest.mark.parametrize("method", ["plain", "batched"])
+def test_query_range_shards_reassemble_the_join(ctx, titles_sets, method):
+    """A join split into query ranges (the multi-GPU sharding) gives the same pairs and counters."""
+    from new_fgssjoin_b200.shard import shard_ranges
+    s = titles_sets
+    ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, 0.7)
+    parts = [ctx.selfjoin(s, 0.7, method=method, query_range=r) for r in shard_ranges(s.len, 3)]
+    assert np.array_equal(np.concatenate([p.q for p in parts]), ref["q"])
+    assert np.array_equal(np.concatenate([p.s for p in parts]), ref["s"])
+    assert sum(p.stats["candidates"] for p in parts) == st["candidates"]
+    assert sum(p.stats["intersections"] for p in parts) == st["intersections"]
