@@ -11,7 +11,8 @@ counter, identical for every method) of the batched + learned form; the plain
 per-stage form is timed on the same step and reported beside it, with a check
 that both pair sets are identical.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload titles100k|heavy1m]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload titles100k|heavy1m|titles18k|heavy300k]
+                 [--thresholds 0.7,0.9] [--no-model] [--no-tune] [--no-cpu-baseline]
   python bench.py --impl reference ...   # the CPU restatement of the reference algorithm
 """
 import argparse
@@ -30,6 +31,7 @@ WORKLOADS = {
     "titles100k": dict(kind="titles", n=100_000, seed=2, thresholds=[0.5, 0.6, 0.7, 0.8, 0.9]),
     "heavy1m": dict(kind="heavy", n=1_000_000, seed=3, thresholds=[0.7]),
     "titles18k": dict(kind="titles", n=18_000, seed=1, thresholds=[0.9]),
+    "heavy300k": dict(kind="heavy", n=300_000, seed=4, thresholds=[0.7]),  # profiling size: > L2, a few GB
 }
 
 
@@ -152,8 +154,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-model", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--thresholds", type=str, default=None, help="comma-separated, overrides the workload's")
     args = ap.parse_args()
-    w = WORKLOADS[args.workload]
+    w = dict(WORKLOADS[args.workload])
+    if args.thresholds:
+        w["thresholds"] = [float(x) for x in args.thresholds.split(",")]
     if args.impl == "reference":
         return run_reference(args, w)
 

@@ -74,6 +74,49 @@ __global__ void k_items(const uint64_t* __restrict__ pre, uint32_t n, uint64_t t
     }
 }
 
+// Item sort keys: ~cost (so ascending order = descending cost), value = item index.
+__global__ void k_item_keys(const uint64_t* __restrict__ pre, uint32_t n, uint64_t total, const uint4* __restrict__ items,
+                            uint32_t K, uint32_t base, uint64_t* __restrict__ key, uint32_t* __restrict__ val) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+        const uint4 it = items[k];
+        const uint64_t b = it.y < n ? pre[it.y] : total;
+        const uint64_t e = it.z < n ? pre[it.z] : total;
+        key[base + k] = ~(e - b);
+        val[base + k] = base + k;
+    }
+}
+
+__global__ void k_permute_items(const uint4* __restrict__ items, const uint32_t* __restrict__ order, uint64_t n,
+                                uint4* __restrict__ out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = items[order[i]];
+}
+
+template <int NT, int HLOG, int RT>
+static int resident_ctas(Ctx& c) {
+    int occ = 0;
+    FGSS_CK(cudaFuncSetAttribute(k_fused<NT, HLOG, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)FusedLayout<HLOG>::bytes));
+    FGSS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused<NT, HLOG, RT>, NT, FusedLayout<HLOG>::bytes));
+    return std::max(occ, 1) * c.num_sms;
+}
+
+int fused_resident_ctas(Ctx& c, const TuneEntry& te) {
+#define FGSS_R(NT, HL, RT) \
+    if (te.threads == NT && te.hash_log2 == HL && te.regs_rt == RT) return resident_ctas<NT, HL, RT>(c);
+    FGSS_R(64, 9, 1024)
+    FGSS_R(64, 9, 768)
+    FGSS_R(64, 9, 512)
+    FGSS_R(64, 10, 1024)
+    FGSS_R(128, 9, 1024)
+    FGSS_R(128, 10, 1024)
+    FGSS_R(128, 10, 768)
+    FGSS_R(128, 11, 768)
+    FGSS_R(256, 11, 768)
+#undef FGSS_R
+    return resident_ctas<64, 9, 768>(c);
+}
+
 template <int NT, int HLOG, int RT>
 static void launch_fused(Ctx& c, const JoinArgs* d_args, const FusedArgs* d_fargs, const uint4* items,
                          uint32_t n_items, uint32_t* counter, int ctas_per_sm) {
@@ -152,8 +195,16 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
     std::vector<uint64_t*> pre(nj);
     FGSS_CK(cudaMemsetAsync(d_tot, 0, (nj * 2 + 2) * 8, c.stream));
     std::vector<FusedArgs> hf(nj);
+    // one launch shape for the batch: the tuned shape of its most expensive
+    // join (the lowest threshold, then the most records)
+    size_t lead = 0;
+    for (size_t i = 1; i < nj; i++)
+        if (joins[i]->t < joins[lead]->t ||
+            (joins[i]->t == joins[lead]->t && joins[i]->in.n_sets > joins[lead]->in.n_sets))
+            lead = i;
     const TuneEntry te = c.tune_force ? *c.tune_force
-                                      : tune_lookup(c, tune_key(joins[0]->in.n_sets, joins[0]->in.n_tokens, joins[0]->t));
+                                      : tune_lookup(c, tune_key(joins[lead]->in.n_sets, joins[lead]->in.n_tokens,
+                                                                joins[lead]->t));
     const uint32_t cap_entries = (1u << te.hash_log2) / 2;  // chunk capacity of the chosen kernel shape
     for (size_t i = 0; i < nj; i++) {
         JoinState& J = *joins[i];
@@ -205,7 +256,9 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
     uint64_t grand = 0;
     for (size_t i = 0; i < nj; i++) grand += htot[i];
     // items: ~16 per resident CTA over the whole batch, split by cost share
-    const uint64_t want = (uint64_t)16 * c.num_sms * std::max(1, te.ctas_per_sm);
+    // ~32 items per resident CTA over the whole batch, split by cost share and
+    // handed out longest first, so the dynamic queue ends with short items
+    const uint64_t want = (uint64_t)32 * fused_resident_ctas(c, te);
     std::vector<uint32_t> K(nj, 0);
     uint64_t nitems = 0;
     for (size_t i = 0; i < nj; i++) {
@@ -225,6 +278,24 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
                                                             (uint32_t)i, items + off);
         FGSS_LAUNCH_CK();
         off += K[i];
+    }
+    if (nitems > 1) {
+        // longest-processing-time order: sort items by descending cost
+        uint64_t* ikey = c.devT<uint64_t>("b.ikey", nitems + 1);
+        uint32_t* ival = c.devT<uint32_t>("b.ival", nitems + 1);
+        uint4* sorted = c.devT<uint4>("b.items2", nitems + 1);
+        uint64_t off2 = 0;
+        for (size_t i = 0; i < nj; i++) {
+            if (!K[i]) continue;
+            k_item_keys<<<grid_for(K[i], 128), 128, 0, c.stream>>>(pre[i], (uint32_t)joins[i]->in.n_sets, htot[i],
+                                                                    items + off2, K[i], (uint32_t)off2, ikey, ival);
+            FGSS_LAUNCH_CK();
+            off2 += K[i];
+        }
+        radix_sort<uint64_t, uint32_t>(c, ikey, ival, nitems, nullptr, 0, 64, "b.isort");
+        k_permute_items<<<grid_for(nitems, 128), 128, 0, c.stream>>>(items, ival, nitems, sorted);
+        FGSS_LAUNCH_CK();
+        items = sorted;
     }
     // result buffers: the learned estimate (x1.5 + slack) or the last size seen
     JoinArgs* d_args = c.devT<JoinArgs>("b.args", nj);
