@@ -55,8 +55,9 @@ __global__ void k_features(JoinArgs a, float t, float* __restrict__ feat, uint32
 
 // Work items of one join: item k = queries with exclusive cost prefix in
 // [k*target, (k+1)*target).
-__global__ void k_items(const uint64_t* __restrict__ pre, uint32_t n, uint64_t total, uint32_t K, uint32_t join,
-                        uint4* __restrict__ items) {
+__global__ void k_items(const uint64_t* __restrict__ pre, uint32_t n, const uint64_t* __restrict__ d_total, uint32_t K,
+                        uint32_t join, uint4* __restrict__ items) {
+    const uint64_t total = *d_total;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
         uint64_t target = (total + K - 1) / K;
         auto first_ge = [&](uint64_t x) {
@@ -75,8 +76,10 @@ __global__ void k_items(const uint64_t* __restrict__ pre, uint32_t n, uint64_t t
 }
 
 // Item sort keys: ~cost (so ascending order = descending cost), value = item index.
-__global__ void k_item_keys(const uint64_t* __restrict__ pre, uint32_t n, uint64_t total, const uint4* __restrict__ items,
-                            uint32_t K, uint32_t base, uint64_t* __restrict__ key, uint32_t* __restrict__ val) {
+__global__ void k_item_keys(const uint64_t* __restrict__ pre, uint32_t n, const uint64_t* __restrict__ d_total,
+                            const uint4* __restrict__ items, uint32_t K, uint32_t base, uint64_t* __restrict__ key,
+                            uint32_t* __restrict__ val) {
+    const uint64_t total = *d_total;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
         const uint4 it = items[k];
         const uint64_t b = it.y < n ? pre[it.y] : total;
@@ -189,22 +192,33 @@ __global__ void k_clear_filter_state(uint32_t* status, unsigned long long* stats
 }
 
 // Runs the fused filter+verify over every join (their index built already).
-void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_model) {
+//
+// With a plan in record mode the host-side decisions of this run (launch
+// shape, work items per join, result capacities, heavy-path slots, grid) are
+// kept; in capture mode (plan->capture) the same device work is issued with
+// those decisions and without any host synchronization, so the stream can be
+// captured into a CUDA graph and replayed on later calls.
+void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_model, BatchPlan* plan) {
     const size_t nj = joins.size();
-    uint64_t* d_tot = c.devT<uint64_t>("b.tot", nj * 2 + 2);
+    const bool capture = plan && plan->capture;
+    uint64_t* d_tot = c.devT<uint64_t>(c.bpfx + "b.tot", nj * 2 + 2);
     std::vector<uint64_t*> pre(nj);
     FGSS_CK(cudaMemsetAsync(d_tot, 0, (nj * 2 + 2) * 8, c.stream));
-    std::vector<FusedArgs> hf(nj);
-    // one launch shape for the batch: the tuned shape of its most expensive
-    // join (the lowest threshold, then the most records)
-    size_t lead = 0;
-    for (size_t i = 1; i < nj; i++)
-        if (joins[i]->t < joins[lead]->t ||
-            (joins[i]->t == joins[lead]->t && joins[i]->in.n_sets > joins[lead]->in.n_sets))
-            lead = i;
-    const TuneEntry te = c.tune_force ? *c.tune_force
-                                      : tune_lookup(c, tune_key(joins[lead]->in.n_sets, joins[lead]->in.n_tokens,
-                                                                joins[lead]->t));
+    FusedArgs* hf = c.pinnedT<FusedArgs>(c.bpfx + "b.hf", nj);
+    TuneEntry te;
+    if (capture) {
+        te = plan->te;
+    } else {
+        // one launch shape for the batch: the tuned shape of its most expensive
+        // join (the lowest threshold, then the most records)
+        size_t lead = 0;
+        for (size_t i = 1; i < nj; i++)
+            if (joins[i]->t < joins[lead]->t ||
+                (joins[i]->t == joins[lead]->t && joins[i]->in.n_sets > joins[lead]->in.n_sets))
+                lead = i;
+        te = c.tune_force ? *c.tune_force
+                          : tune_lookup(c, tune_key(joins[lead]->in.n_sets, joins[lead]->in.n_tokens, joins[lead]->t));
+    }
     const uint32_t cap_entries = (1u << te.hash_log2) / 2;  // chunk capacity of the chosen kernel shape
     for (size_t i = 0; i < nj; i++) {
         JoinState& J = *joins[i];
@@ -217,16 +231,20 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         uint32_t* wtot = c.devT<uint32_t>(J.pfx("wtot"), n + 1);
         uint32_t* pred = c.devT<uint32_t>(J.pfx("pred"), n + 1);
         pre[i] = c.devT<uint64_t>(J.pfx("cpre"), n + 1);
-        hf[i].poff = poff;
-        hf[i].win = win;
-        hf[i].smin = J.lut.smin;
-        if (n == 0) continue;
-        // windows of every probe token (exact per-query work), then features and the learned estimate
-        exclusive_scan<uint32_t>(c, J.pcnt, poff, n, nullptr, (uint32_t*)nullptr, J.pfx("scan.p").c_str());
         uint4* meta = c.devT<uint4>(J.pfx("meta"), n + 1);
         uint2* qchunk = c.devT<uint2>(J.pfx("qchunk"), n + 1);
         const uint64_t cbuf_cap = 2 * J.in.n_tokens + (1u << 20);  // overflowing queries bisect instead
         uint32_t* cbuf = c.devT<uint32_t>(J.pfx("cbuf"), cbuf_cap);
+        hf[i].poff = poff;
+        hf[i].win = win;
+        hf[i].smin = J.lut.smin;
+        hf[i].meta = meta;
+        hf[i].qchunk = qchunk;
+        hf[i].cbuf = cbuf;
+        if (n == 0) continue;
+        // windows of every probe token (exact per-query work), chunk splits, then
+        // features and the learned estimate, then the work-item cost prefix
+        exclusive_scan<uint32_t>(c, J.pcnt, poff, n, nullptr, (uint32_t*)nullptr, J.pfx("scan.p").c_str());
         unsigned long long* cused = reinterpret_cast<unsigned long long*>(J.status + 4);
         FGSS_CK(cudaMemsetAsync(cused, 0, 8, c.stream));
         k_windows<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wtot, meta);
@@ -234,9 +252,6 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         k_chunks<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wtot, cap_entries,
                                                                             qchunk, cbuf, cbuf_cap, cused);
         FGSS_LAUNCH_CK();
-        hf[i].meta = meta;
-        hf[i].qchunk = qchunk;
-        hf[i].cbuf = cbuf;
         const bool model = use_model && c.model && !J.res_cap_hint;
         if (model) {
             k_features<<<grid_for(n * 32, 256, c.num_sms * 32), 256, 0, c.stream>>>(J.args, J.t, feat, fcost);
@@ -248,75 +263,83 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         FGSS_LAUNCH_CK();
         exclusive_scan<uint64_t>(c, cost, pre[i], n, nullptr, &d_tot[i], J.pfx("scan.cost").c_str());
     }
-    FusedArgs* d_fargs = c.devT<FusedArgs>("b.fargs", nj);
-    FGSS_CK(cudaMemcpyAsync(d_fargs, hf.data(), nj * sizeof(FusedArgs), cudaMemcpyHostToDevice, c.stream));
-    std::vector<uint64_t> htot(2 * nj + 2);
-    FGSS_CK(cudaMemcpyAsync(htot.data(), d_tot, (2 * nj + 2) * 8, cudaMemcpyDeviceToHost, c.stream));
-    c.sync();
-    uint64_t grand = 0;
-    for (size_t i = 0; i < nj; i++) grand += htot[i];
-    // items: ~16 per resident CTA over the whole batch, split by cost share
-    // ~32 items per resident CTA over the whole batch, split by cost share and
-    // handed out longest first, so the dynamic queue ends with short items
-    const uint64_t want = (uint64_t)32 * fused_resident_ctas(c, te);
+    FusedArgs* d_fargs = c.devT<FusedArgs>(c.bpfx + "b.fargs", nj);
+    FGSS_CK(cudaMemcpyAsync(d_fargs, hf, nj * sizeof(FusedArgs), cudaMemcpyHostToDevice, c.stream));
     std::vector<uint32_t> K(nj, 0);
     uint64_t nitems = 0;
-    for (size_t i = 0; i < nj; i++) {
-        const uint64_t n = joins[i]->in.n_sets;
-        if (n == 0) continue;
-        uint64_t k = grand ? (want * htot[i] + grand - 1) / grand : 1;
-        k = std::max<uint64_t>(1, std::min<uint64_t>(k, n));
-        K[i] = (uint32_t)k;
-        nitems += k;
+    std::vector<uint64_t> htot(2 * nj + 2, 0);
+    if (capture) {
+        K = plan->K;
+        nitems = plan->nitems;
+    } else {
+        FGSS_CK(cudaMemcpyAsync(htot.data(), d_tot, (2 * nj + 2) * 8, cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+        uint64_t grand = 0;
+        for (size_t i = 0; i < nj; i++) grand += htot[i];
+        // ~32 items per resident CTA over the whole batch, split by cost share and
+        // handed out longest first, so the dynamic queue ends with short items
+        const uint64_t want = (uint64_t)32 * fused_resident_ctas(c, te);
+        for (size_t i = 0; i < nj; i++) {
+            const uint64_t n = joins[i]->in.n_sets;
+            if (n == 0) continue;
+            uint64_t k = grand ? (want * htot[i] + grand - 1) / grand : 1;
+            k = std::max<uint64_t>(1, std::min<uint64_t>(k, n));
+            K[i] = (uint32_t)k;
+            nitems += k;
+        }
     }
-    uint4* items = c.devT<uint4>("b.items", nitems + 1);
+    uint4* items = c.devT<uint4>(c.bpfx + "b.items", nitems + 1);
     uint64_t off = 0;
     for (size_t i = 0; i < nj; i++) {
         if (!K[i]) continue;
         JoinState& J = *joins[i];
-        k_items<<<grid_for(K[i], 128), 128, 0, c.stream>>>(pre[i], (uint32_t)J.in.n_sets, htot[i], K[i],
+        k_items<<<grid_for(K[i], 128), 128, 0, c.stream>>>(pre[i], (uint32_t)J.in.n_sets, &d_tot[i], K[i],
                                                             (uint32_t)i, items + off);
         FGSS_LAUNCH_CK();
         off += K[i];
     }
     if (nitems > 1) {
         // longest-processing-time order: sort items by descending cost
-        uint64_t* ikey = c.devT<uint64_t>("b.ikey", nitems + 1);
-        uint32_t* ival = c.devT<uint32_t>("b.ival", nitems + 1);
-        uint4* sorted = c.devT<uint4>("b.items2", nitems + 1);
+        uint64_t* ikey = c.devT<uint64_t>(c.bpfx + "b.ikey", nitems + 1);
+        uint32_t* ival = c.devT<uint32_t>(c.bpfx + "b.ival", nitems + 1);
+        uint4* sorted = c.devT<uint4>(c.bpfx + "b.items2", nitems + 1);
         uint64_t off2 = 0;
         for (size_t i = 0; i < nj; i++) {
             if (!K[i]) continue;
-            k_item_keys<<<grid_for(K[i], 128), 128, 0, c.stream>>>(pre[i], (uint32_t)joins[i]->in.n_sets, htot[i],
+            k_item_keys<<<grid_for(K[i], 128), 128, 0, c.stream>>>(pre[i], (uint32_t)joins[i]->in.n_sets, &d_tot[i],
                                                                     items + off2, K[i], (uint32_t)off2, ikey, ival);
             FGSS_LAUNCH_CK();
             off2 += K[i];
         }
-        radix_sort<uint64_t, uint32_t>(c, ikey, ival, nitems, nullptr, 0, 64, "b.isort");
+        radix_sort<uint64_t, uint32_t>(c, ikey, ival, nitems, nullptr, 0, 64, (c.bpfx + "b.isort").c_str());
         k_permute_items<<<grid_for(nitems, 128), 128, 0, c.stream>>>(items, ival, nitems, sorted);
         FGSS_LAUNCH_CK();
         items = sorted;
     }
-    // result buffers: the learned estimate (x1.5 + slack) or the last size seen
-    JoinArgs* d_args = c.devT<JoinArgs>("b.args", nj);
-    std::vector<JoinArgs> hargs(nj);
+    // result buffers: the caller's size, the learned estimate (x1.5 + slack),
+    // or the last size seen for this slot
+    JoinArgs* d_args = c.devT<JoinArgs>(c.bpfx + "b.args", nj);
+    JoinArgs* hargs = c.pinnedT<JoinArgs>(c.bpfx + "b.hargs", nj);
     for (size_t i = 0; i < nj; i++) {
         JoinState& J = *joins[i];
         const uint64_t n = J.in.n_sets;
         uint64_t cap;
-        auto itc = c.tune.find(J.pfx("rescap"));
-        const uint64_t last = itc != c.tune.end() ? (uint64_t)itc->second.ctas_per_sm : 0;
-        if (J.res_cap_hint) {
-            cap = J.res_cap_hint;
-        } else if (J.res_cap_user) {
-            cap = J.res_cap_user;
-        } else if (use_model && c.model) {
-            // the model's predicted result count, x1.5 + slack
-            cap = (uint64_t)((double)htot[nj + i] * 1.5) + 4096;  // predicted results x 1.5 + slack
+        if (capture) {
+            cap = plan->res_cap[i];
         } else {
-            cap = std::max<uint64_t>(n + 4096, last);
+            auto itc = c.tune.find(J.pfx("rescap"));
+            const uint64_t last = itc != c.tune.end() ? (uint64_t)itc->second.ctas_per_sm : 0;
+            if (J.res_cap_hint) {
+                cap = J.res_cap_hint;
+            } else if (J.res_cap_user) {
+                cap = J.res_cap_user;
+            } else if (use_model && c.model) {
+                cap = (uint64_t)((double)htot[nj + i] * 1.5) + 4096;  // predicted results x 1.5 + slack
+            } else {
+                cap = std::max<uint64_t>(n + 4096, last);
+            }
+            cap = std::min<uint64_t>(cap, 0xfffffff0ull);
         }
-        cap = std::min<uint64_t>(cap, 0xfffffff0ull);
         JoinArgs& a = J.args;
         a.res_cap = (uint32_t)cap;
         a.res_q = c.devT<uint32_t>(J.pfx("res.q"), cap + 1);
@@ -326,35 +349,70 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         FGSS_CK(cudaMemsetAsync(a.heavy_count, 0, 8, c.stream));  // heavy_count + res_count
         hargs[i] = a;
     }
-    FGSS_CK(cudaMemcpyAsync(d_args, hargs.data(), nj * sizeof(JoinArgs), cudaMemcpyHostToDevice, c.stream));
-    uint32_t* counter = c.devT<uint32_t>("b.counter", 4 + nj);
+    FGSS_CK(cudaMemcpyAsync(d_args, hargs, nj * sizeof(JoinArgs), cudaMemcpyHostToDevice, c.stream));
+    uint32_t* counter = c.devT<uint32_t>(c.bpfx + "b.counter", 4 + nj);
     FGSS_CK(cudaMemsetAsync(counter, 0, (4 + nj) * 4, c.stream));
     FGSS_CK(cudaEventRecord(c.ev[4], c.stream));
     if (nitems) fused_launch(c, te, d_args, d_fargs, items, (uint32_t)nitems, counter);
     FGSS_CK(cudaEventRecord(c.ev[5], c.stream));
     c.probe_timed = true;
-    // heavy queries: read the queue sizes, one persistent launch per join
-    std::vector<uint32_t> hq(2 * nj);
-    uint32_t* hbuf = c.pinnedT<uint32_t>("b.hq", 2 * nj + 2);
-    for (size_t i = 0; i < nj; i++)
-        FGSS_CK(cudaMemcpyAsync(hbuf + 2 * i, joins[i]->status + 2, 8, cudaMemcpyDeviceToHost, c.stream));
-    c.sync();
+    // heavy queries: one persistent launch per join.  Eagerly only when some
+    // were queued; under a plan always, with scratch for a fixed slot count
+    // (a launch with an empty queue returns at once).
+    uint32_t* hbuf = c.pinnedT<uint32_t>(c.bpfx + "b.hq", 2 * nj + 2);
+    if (!capture) {
+        for (size_t i = 0; i < nj; i++)
+            FGSS_CK(cudaMemcpyAsync(hbuf + 2 * i, joins[i]->status + 2, 8, cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+    }
     for (size_t i = 0; i < nj; i++) {
-        uint32_t nh = hbuf[2 * i];
-        if (!nh) continue;
         JoinState& J = *joins[i];
-        uint32_t slots = std::min<uint32_t>(nh, (uint32_t)c.num_sms);
+        uint32_t slots;
+        if (capture) {
+            slots = plan->heavy_slots[i];
+        } else {
+            const uint32_t nh = hbuf[2 * i];
+            slots = plan ? std::min<uint32_t>((uint32_t)std::max<uint64_t>(J.in.n_sets, 1), (uint32_t)c.num_sms)
+                         : std::min<uint32_t>(nh, (uint32_t)c.num_sms);
+            if (!nh && !plan) slots = 0;
+        }
+        if (!slots) continue;
         uint64_t words = 4 * J.in.n_sets + 65536 + 65537;
         words = (words + 63) & ~63ull;
-        const std::string name = "heavy.scratch";
+        const std::string name = c.bpfx + "heavy.scratch";
         auto it = c.bufs.find(name);
-        size_t need = words * slots * 4;
-        bool grow = it == c.bufs.end() || it->second.bytes < need;
+        const size_t need = words * slots * 4;
+        const bool grow = it == c.bufs.end() || it->second.bytes < need;
+        if (grow && capture) fail(FGSS_ERR_CUDA, "heavy scratch would grow inside a graph capture");
         uint32_t* scratch = (uint32_t*)c.dev(name, need);
         if (grow) FGSS_CK(cudaMemsetAsync(scratch, 0, c.bufs[name].bytes, c.stream));
         k_probe_heavy<MODE_FUSED, 512><<<slots, 512, 0, c.stream>>>(d_args, (uint32_t)i, scratch, words,
                                                                     counter + 4 + i);
         FGSS_LAUNCH_CK();
+    }
+    if (plan && !capture) {
+        plan->te = te;
+        plan->K = K;
+        plan->nitems = nitems;
+        plan->heavy_slots.assign(nj, 0);
+        for (size_t i = 0; i < nj; i++)
+            plan->heavy_slots[i] =
+                std::min<uint32_t>((uint32_t)std::max<uint64_t>(joins[i]->in.n_sets, 1), (uint32_t)c.num_sms);
+        plan->res_cap.assign(nj, 0);
+    }
+    if (capture) {
+        // results sorted at full capacity; the host reads the counts after replay
+        for (size_t i = 0; i < nj; i++) {
+            JoinState& J = *joins[i];
+            uint64_t* keys = c.devT<uint64_t>(J.pfx("rkey"), (uint64_t)J.args.res_cap + 1);
+            uint32_t* vals = c.devT<uint32_t>(J.pfx("rval"), (uint64_t)J.args.res_cap + 1);
+            J.d_nres = c.devT<uint64_t>(J.pfx("nres"), 2);
+            k_result_keys<<<grid_for(J.args.res_cap, 256, c.num_sms * 32), 256, 0, c.stream>>>(
+                J.args.res_q, J.args.res_s, J.args.res_o, J.status + 3, J.args.res_cap, keys, vals, J.d_nres);
+            FGSS_LAUNCH_CK();
+            join_output(c, J, keys, vals, J.d_nres, J.args.res_cap);
+        }
+        return;
     }
     // results: overflow -> exact re-run of that join with the exact capacity
     for (size_t i = 0; i < nj; i++)
@@ -371,9 +429,11 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
             k_clear_filter_state<<<1, 32, 0, c.stream>>>(J.status, J.stats);
             FGSS_LAUNCH_CK();
             std::vector<JoinState*> one{&J};
-            batched_filter_verify(c, one, false);
+            batched_filter_verify(c, one, false, nullptr);
+            if (plan) plan->valid = false;  // a batch that overflowed is not captured
             continue;
         }
+        if (plan) plan->res_cap[i] = J.args.res_cap;
         // remember a sufficient capacity for the next call on this slot
         J.res_cap_hint = 0;
         c.tune[J.pfx("rescap")].ctas_per_sm = (int)std::min<uint64_t>((uint64_t)got + got / 4 + 1024, 0x7fffffff);

@@ -42,6 +42,11 @@ struct Ctx {
     std::map<std::string, DevBuf> host_bufs;  // pinned
     std::map<std::string, TuneEntry> tune;
     const TuneEntry* tune_force = nullptr;  // set by the autotuner while it times a shape
+    // Buffer-name namespace of the batch-level buffers: "" normally, a graph's
+    // own "g<id>." while a graph-eligible batch is recorded or captured, so no
+    // later call can move a buffer a captured graph points to.
+    std::string bpfx;
+    struct GraphCache* graphs = nullptr;  // captured batched pipelines (api.cu)
     fgss_model* model = nullptr;
     cudaEvent_t ev[8] = {};
     bool probe_timed = false;  // ev[4]..ev[5] bracket the last fused filter+verify launch
@@ -83,7 +88,17 @@ struct Ctx {
         return static_cast<T*>(pinned(name, count * sizeof(T)));
     }
     void sync() { FGSS_CK(cudaStreamSynchronize(stream)); }
-    void release_all();
+    // Frees every pooled device buffer whose name starts with `prefix`.
+    void release_prefix(const std::string& prefix) {
+        for (auto it = bufs.begin(); it != bufs.end();) {
+            if (it->first.compare(0, prefix.size(), prefix) == 0) {
+                if (it->second.p) cudaFree(it->second.p);
+                it = bufs.erase(it);
+            } else {
+                ++it;
+            }
+        }
+    }
 };
 
 }  // namespace fgss

@@ -54,7 +54,8 @@ struct JoinState {
     uint32_t status_host = 0;
     unsigned long long stats_host[SS_N] = {};
     std::vector<uint32_t> cand_host;  // (q, s, partial) triples when requested
-    std::string pfx(const char* name) const { return "j" + std::to_string(slot) + "." + name; }
+    std::string ns;                   // buffer-name namespace ("" or a captured graph's own "g<id>.")
+    std::string pfx(const char* name) const { return ns + "j" + std::to_string(slot) + "." + name; }
 };
 
 // Stage drivers (join.cu)
@@ -65,12 +66,18 @@ void join_features(Ctx& c, JoinState& J, float* d_feat);
 void join_finish_status(Ctx& c, JoinState& J);  // D2H of status + stats, throws on bad input
 void join_output(Ctx& c, JoinState& J, uint64_t* keys, uint32_t* vals, const uint64_t* d_n, uint64_t n_cap);
 
-// Fused persistent filter+verify over many joins at once (batch.cu)
+// Host-side decisions of one batched run, recorded eagerly and reused when the
+// same batch is captured into a CUDA graph (batch.cu).
 struct BatchPlan {
-    std::vector<uint32_t> res_cap;   // per join
-    bool use_model = false;
+    bool capture = false;             // issue device work only, with these decisions
+    bool valid = true;                // false: the run overflowed; do not capture it
+    TuneEntry te;
+    std::vector<uint32_t> K;          // work items per join
+    uint64_t nitems = 0;
+    std::vector<uint64_t> res_cap;    // result slots per join
+    std::vector<uint32_t> heavy_slots;
 };
-void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_model);
+void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_model, BatchPlan* plan = nullptr);
 
 // Autotuner (tune.cu): workload class of a join, the shapes to try, the
 // cache file.
