@@ -150,6 +150,7 @@ typedef struct fgss_join_opts {
                                  Too small a value only costs an exact re-run. */
     uint64_t query_begin;   /* only queries (first records of pairs) in [query_begin, query_end) */
     uint64_t query_end;     /* are processed; 0, 0 = all.  Used to shard one join over GPUs. */
+    int no_graph;           /* batched method on device inputs: 1 = never capture / replay a CUDA graph */
 } fgss_join_opts;
 
 void fgss_join_opts_default(fgss_join_opts* o);

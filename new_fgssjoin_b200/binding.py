@@ -51,7 +51,7 @@ class _JoinOpts(ctypes.Structure):
     _fields_ = [("threshold", ctypes.c_float), ("bounds", ctypes.c_int), ("method", ctypes.c_int),
                 ("out_on_device", ctypes.c_int), ("want_candidates", ctypes.c_int), ("use_model", ctypes.c_int),
                 ("result_capacity", ctypes.c_uint64), ("query_begin", ctypes.c_uint64),
-                ("query_end", ctypes.c_uint64)]
+                ("query_end", ctypes.c_uint64), ("no_graph", ctypes.c_int)]
 
 
 class _Stats(ctypes.Structure):

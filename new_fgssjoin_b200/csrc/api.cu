@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <map>
 #include <memory>
 #include <vector>
 
@@ -111,36 +112,8 @@ void export_pairs(Ctx& c, JoinState& J, const fgss_join_opts& o, fgss_pairs* out
     c.sync();
 }
 
-void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, int n, fgss_pairs* outs,
-               fgss_stats* stats) {
-    if (n <= 0) return;
-    if (!sets || !opts || !outs) fail(FGSS_ERR_INVALID, "null argument");
-    std::vector<std::unique_ptr<JoinState>> js(n);
+void report_stats(Ctx& c, std::vector<JoinState*>& js, fgss_stats* stats, unsigned long long launches, int n) {
     cudaEvent_t* ev = c.ev;
-    const unsigned long long launches0 = launch_counter();
-    c.probe_timed = false;
-    FGSS_CK(cudaEventRecord(ev[0], c.stream));
-    for (int i = 0; i < n; i++) {
-        js[i].reset(new JoinState());
-        join_setup(c, *js[i], sets[i], opts[i], i);
-        join_index(c, *js[i]);
-    }
-    FGSS_CK(cudaEventRecord(ev[1], c.stream));
-    bool batched = false;
-    for (int i = 0; i < n; i++) batched |= opts[i].method == FGSS_METHOD_BATCHED;
-    if (batched) {
-        std::vector<JoinState*> v;
-        for (int i = 0; i < n; i++) v.push_back(js[i].get());
-        batched_filter_verify(c, v, opts[0].use_model != 0);
-        if (opts[0].want_candidates) fail(FGSS_ERR_INVALID, "want_candidates needs the plain method");
-    } else {
-        for (int i = 0; i < n; i++) join_plain_filter_verify(c, *js[i], opts[i].want_candidates != 0);
-    }
-    FGSS_CK(cudaEventRecord(ev[2], c.stream));
-    for (int i = 0; i < n; i++) {
-        join_finish_status(c, *js[i]);
-        export_pairs(c, *js[i], opts[i], &outs[i]);
-    }
     FGSS_CK(cudaEventRecord(ev[3], c.stream));
     FGSS_CK(cudaEventSynchronize(ev[3]));
     float t_idx = 0, t_fv = 0, t_out = 0;
@@ -149,12 +122,15 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
     FGSS_CK(cudaEventElapsedTime(&t_out, ev[2], ev[3]));
     float t_probe = 0;
     if (c.probe_timed) FGSS_CK(cudaEventElapsedTime(&t_probe, ev[4], ev[5]));
-    const unsigned long long launches = launch_counter() - launches0;
     if (stats) {
+        uint64_t* he = c.pinnedT<uint64_t>("h.E", (size_t)n + 1);
+        for (int i = 0; i < n; i++)
+            FGSS_CK(cudaMemcpyAsync(he + i, js[i]->d_e, 8, cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
         for (int i = 0; i < n; i++) {
             memset(&stats[i], 0, sizeof(fgss_stats));
             fill_stats(*js[i], &stats[i]);
-            stats[i].index_entries = 0;
+            stats[i].index_entries = he[i];
             stats[i].ms_index = t_idx;
             stats[i].ms_filter = t_fv;
             stats[i].ms_output = t_out;
@@ -162,16 +138,219 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
             stats[i].ms_probe = t_probe;
             stats[i].launches = launches;
         }
-        // index entries: device count
-        for (int i = 0; i < n; i++) {
-            uint64_t e = 0;
-            FGSS_CK(cudaMemcpy(&e, js[i]->d_e, 8, cudaMemcpyDeviceToHost));
-            stats[i].index_entries = e;
-        }
     }
     if (c.verbose)
         fprintf(stderr, "[fgss] joins=%d index %.3f ms, filter+verify %.3f ms, output %.3f ms\n", n, t_idx, t_fv,
                 t_out);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- graphs
+//
+// A batched call whose inputs are all on the device is recorded eagerly the
+// first time (BatchPlan) and then captured, index build included, into one
+// CUDA graph under its own buffer namespace.  A later call with the same
+// inputs (device pointers, sizes, thresholds, options) re-validates its input
+// eagerly, replays the graph, and falls back to the eager path if any
+// presized buffer overflowed.
+namespace fgss {
+struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    std::string ns;
+    std::vector<std::unique_ptr<JoinState>> joins;
+    unsigned long long launches = 0;  // kernels inside the graph
+    uint64_t stamp = 0;
+};
+
+struct GraphCache {
+    std::map<std::string, std::unique_ptr<GraphEntry>> entries;
+    uint64_t next_id = 0, clock = 0;
+};
+}  // namespace fgss
+
+namespace {
+
+constexpr size_t kMaxGraphs = 4;
+
+void drop_graph(Ctx& c, std::unique_ptr<GraphEntry>& g) {
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    c.release_prefix(g->ns);
+    g.reset();
+}
+
+}  // namespace
+
+// Drops every captured batch (after the tuned shapes or the model changed).
+void fgss::clear_graphs(Ctx& c) {
+    if (!c.graphs) return;
+    cudaStreamSynchronize(c.stream);
+    for (auto& kv : c.graphs->entries) drop_graph(c, kv.second);
+    c.graphs->entries.clear();
+}
+
+namespace {
+
+std::string graph_key(const fgss_sets_view* sets, const fgss_join_opts* opts, int n) {
+    std::string k;
+    char buf[256];
+    for (int i = 0; i < n; i++) {
+        uint32_t tb;
+        memcpy(&tb, &opts[i].threshold, 4);
+        snprintf(buf, sizeof buf, "%p,%p,%p,%p,%llu,%llu,%u|%u,%d,%d,%llu,%llu,%llu;", (const void*)sets[i].id,
+                 (const void*)sets[i].pos, (const void*)sets[i].len, (const void*)sets[i].tokens,
+                 (unsigned long long)sets[i].n_sets, (unsigned long long)sets[i].n_tokens, sets[i].n_terms, tb,
+                 opts[i].bounds, opts[i].use_model, (unsigned long long)opts[i].result_capacity,
+                 (unsigned long long)opts[i].query_begin, (unsigned long long)opts[i].query_end);
+        k += buf;
+    }
+    return k;
+}
+
+// Replays a captured batch; false when its presized buffers overflowed (the
+// caller then runs the exact eager path).
+bool replay_graph(Ctx& c, GraphEntry& g, const fgss_sets_view* sets, const fgss_join_opts* opts, int n,
+                  fgss_pairs* outs, fgss_stats* stats) {
+    c.bpfx = g.ns;
+    c.probe_timed = false;
+    FGSS_CK(cudaEventRecord(c.ev[0], c.stream));
+    for (int i = 0; i < n; i++) {
+        // validation and fresh counters; the captured arguments (result buffers
+        // and capacities) stay as they were recorded
+        const JoinArgs saved = g.joins[i]->args;
+        join_setup(c, *g.joins[i], sets[i], opts[i], i);
+        g.joins[i]->args = saved;
+    }
+    FGSS_CK(cudaEventRecord(c.ev[1], c.stream));
+    FGSS_CK(cudaGraphLaunch(g.exec, c.stream));
+    launch_counter() += g.launches;
+    c.probe_timed = true;
+    FGSS_CK(cudaEventRecord(c.ev[2], c.stream));
+    uint32_t* h = c.pinnedT<uint32_t>(g.ns + "h.st", 4 * (size_t)n + 4);
+    for (int i = 0; i < n; i++)
+        FGSS_CK(cudaMemcpyAsync(h + 4 * i, g.joins[i]->status, 16, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    c.bpfx.clear();
+    for (int i = 0; i < n; i++) {
+        const uint32_t bad = ST_RES_OVERFLOW | ST_HEAVY_OVERFLOW | ST_HASH_FULL;
+        if ((h[4 * i] & bad) || h[4 * i + 3] > g.joins[i]->args.res_cap) return false;
+    }
+    std::vector<JoinState*> v;
+    for (int i = 0; i < n; i++) {
+        JoinState& J = *g.joins[i];
+        J.n_res = h[4 * i + 3];
+        J.overflow_retries = 0;
+        join_finish_status(c, J);
+        export_pairs(c, J, opts[i], &outs[i]);
+        v.push_back(&J);
+    }
+    report_stats(c, v, stats, g.launches, n);
+    return true;
+}
+
+void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, int n, fgss_pairs* outs,
+               fgss_stats* stats) {
+    if (n <= 0) return;
+    if (!sets || !opts || !outs) fail(FGSS_ERR_INVALID, "null argument");
+    bool batched = false;
+    for (int i = 0; i < n; i++) batched |= opts[i].method == FGSS_METHOD_BATCHED;
+    if (batched && opts[0].want_candidates) fail(FGSS_ERR_INVALID, "want_candidates needs the plain method");
+    bool graphable = batched && !c.tune_force && c.graphs;
+    for (int i = 0; i < n; i++) graphable &= sets[i].on_device != 0 && !opts[i].no_graph;
+    std::string gkey;
+    if (graphable) {
+        gkey = graph_key(sets, opts, n);
+        auto it = c.graphs->entries.find(gkey);
+        if (it != c.graphs->entries.end()) {
+            it->second->stamp = ++c.graphs->clock;
+            bool ok = false;
+            try {
+                ok = replay_graph(c, *it->second, sets, opts, n, outs, stats);
+            } catch (...) {
+                c.bpfx.clear();
+                throw;
+            }
+            if (ok) return;
+            for (int i = 0; i < n; i++) fgss_pairs_free(&outs[i]);
+            drop_graph(c, it->second);  // its plan no longer fits the data
+            c.graphs->entries.erase(it);
+        }
+    }
+    std::unique_ptr<GraphEntry> g;
+    if (graphable) {
+        g.reset(new GraphEntry());
+        g->ns = "g" + std::to_string(c.graphs->next_id++) + ".";
+        c.bpfx = g->ns;
+    }
+    std::vector<std::unique_ptr<JoinState>> js(n);
+    cudaEvent_t* ev = c.ev;
+    const unsigned long long launches0 = launch_counter();
+    c.probe_timed = false;
+    BatchPlan plan;
+    try {
+        FGSS_CK(cudaEventRecord(ev[0], c.stream));
+        for (int i = 0; i < n; i++) {
+            js[i].reset(new JoinState());
+            if (g) js[i]->ns = g->ns;
+            join_setup(c, *js[i], sets[i], opts[i], i);
+            join_index(c, *js[i]);
+        }
+        FGSS_CK(cudaEventRecord(ev[1], c.stream));
+        std::vector<JoinState*> v;
+        for (int i = 0; i < n; i++) v.push_back(js[i].get());
+        if (batched) {
+            batched_filter_verify(c, v, opts[0].use_model != 0, g ? &plan : nullptr);
+        } else {
+            for (int i = 0; i < n; i++) join_plain_filter_verify(c, *js[i], opts[i].want_candidates != 0);
+        }
+        FGSS_CK(cudaEventRecord(ev[2], c.stream));
+        for (int i = 0; i < n; i++) {
+            join_finish_status(c, *js[i]);
+            export_pairs(c, *js[i], opts[i], &outs[i]);
+        }
+        report_stats(c, v, stats, launch_counter() - launches0, n);
+        if (g && plan.valid) {
+            // capture the same batch (index build included) for later calls
+            plan.capture = true;
+            const unsigned long long l0 = launch_counter();
+            cudaGraph_t graph = nullptr;
+            FGSS_CK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                for (int i = 0; i < n; i++) join_index(c, *js[i]);
+                batched_filter_verify(c, v, opts[0].use_model != 0, &plan);
+            } catch (...) {
+                cudaStreamEndCapture(c.stream, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            FGSS_CK(cudaStreamEndCapture(c.stream, &graph));
+            const cudaError_t e = cudaGraphInstantiate(&g->exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) fail(FGSS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            g->launches = launch_counter() - l0;
+            launch_counter() = l0;  // captured, not launched
+            g->joins = std::move(js);
+            g->stamp = ++c.graphs->clock;
+            if (c.graphs->entries.size() >= kMaxGraphs) {
+                auto oldest = c.graphs->entries.begin();
+                for (auto it = c.graphs->entries.begin(); it != c.graphs->entries.end(); ++it)
+                    if (it->second->stamp < oldest->second->stamp) oldest = it;
+                drop_graph(c, oldest->second);
+                c.graphs->entries.erase(oldest);
+            }
+            c.graphs->entries[gkey] = std::move(g);
+        } else if (g) {
+            c.release_prefix(g->ns);
+        }
+    } catch (...) {
+        c.bpfx.clear();
+        if (g) {
+            cudaStreamSynchronize(c.stream);
+            c.release_prefix(g->ns);
+        }
+        throw;
+    }
+    c.bpfx.clear();
 }
 
 }  // namespace
@@ -251,6 +430,7 @@ fgss_status fgss_create(fgss_ctx** out, const fgss_options* opt) {
         }
         for (auto& e : c.ev) FGSS_CK(cudaEventCreate(&e));
         tune_load(c);
+        c.graphs = new GraphCache();
     });
     if (st != FGSS_OK) {
         g_err = ctx->c.last_error;
@@ -266,6 +446,9 @@ void fgss_destroy(fgss_ctx* ctx) {
     Ctx& c = ctx->c;
     cudaSetDevice(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);
+    clear_graphs(c);
+    delete c.graphs;
+    c.graphs = nullptr;
     for (auto& kv : c.bufs)
         if (kv.second.p) cudaFree(kv.second.p);
     for (auto& kv : c.host_bufs)
@@ -412,6 +595,7 @@ fgss_status fgss_autotune(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_
         }
         c.tune[key] = win;
         tune_save(c);
+        clear_graphs(c);  // captured batches used the previous shapes
         if (best) {
             best->threads = win.threads;
             best->hash_log2 = win.hash_log2;

@@ -88,4 +88,7 @@ TuneEntry tune_lookup(Ctx& c, const std::string& key);
 void tune_load(Ctx& c);
 void tune_save(Ctx& c);
 
+// Captured batched pipelines (api.cu): dropped when shapes or the model change.
+void clear_graphs(Ctx& c);
+
 }  // namespace fgss

@@ -78,6 +78,7 @@ fgss_status fgss_model_train(fgss_ctx* ctx, const fgss_sets_view* sets, const fl
             res_total += J.n_res;
         }
         c.sync();
+        clear_graphs(c);  // captured batches presized with the previous model
         float loss = model_fit(c, feat, target, off, epochs, lr, seed);
         // calibration of the summed result estimate against the truth
         uint32_t* cost = c.devT<uint32_t>("mt.cost2", off + 1);
@@ -152,6 +153,7 @@ fgss_status fgss_model_load(fgss_ctx* ctx, const char* path) {
     try {
         Ctx& c = ctx->c;
         FGSS_CK(cudaSetDevice(c.device));
+        clear_graphs(c);
         if (!c.model) c.model = new fgss_model();
         c.model->host = p;
         c.model->dev = c.devT<float>("m.P", kParamsAll);

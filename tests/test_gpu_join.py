@@ -227,3 +227,60 @@ def test_query_range_shards_reassemble_the_join(ctx, titles_sets, method):
     assert np.array_equal(np.concatenate([p.s for p in parts]), ref["s"])
     assert sum(p.stats["candidates"] for p in parts) == st["candidates"]
     assert sum(p.stats["intersections"] for p in parts) == st["intersections"]
+
+
+def _device_view(sets):
+    import torch
+    from new_fgssjoin_b200.binding import _View
+    arrs = [torch.from_numpy(a.view(np.int32)).cuda() for a in (sets.id, sets.pos, sets.len, sets.tokens)]
+    v = _View()
+    v.id, v.pos, v.len, v.tokens = [t.data_ptr() for t in arrs]
+    v.n_sets, v.n_tokens, v.n_terms, v.on_device = sets.n_sets, sets.n_tokens, sets.n_terms, 1
+    return v, arrs
+
+
+def test_graph_replay_matches_and_follows_new_contents(ctx):
+    """Batched joins on device inputs are captured into a CUDA graph on the first
+    call and replayed on the next ones: same pairs, and a replay after the input
+    contents changed (same pointers, same sizes) still gives the right pairs."""
+    import torch
+    a = ctx.tokenize(_titles(4000, 71), **datagen.TITLE_TOK)
+    v, arrs = _device_view(a)
+    ts = [0.6, 0.8]
+    refs = [O.join(a.pos, a.len, a.tokens, a.n_terms, t) for t in ts]
+    for call in range(3):  # record + capture, then two replays
+        outs = ctx.selfjoin_batch([v, v], ts)
+        for got, (ref, st) in zip(outs, refs):
+            _check_same(got, ref, st)
+    # new contents in the same buffers: term ids permuted, each record re-sorted
+    perm = np.random.default_rng(5).permutation(a.n_terms).astype(np.uint32)
+    tok = perm[a.tokens]
+    for i in range(a.n_sets):
+        tok[a.pos[i]:a.pos[i] + a.len[i]] = np.sort(tok[a.pos[i]:a.pos[i] + a.len[i]])
+    arrs[3].copy_(torch.from_numpy(tok.view(np.int32)))
+    c = F.Sets(a.id, a.pos, a.len, tok, a.n_terms)
+    refs2 = [O.join(c.pos, c.len, c.tokens, c.n_terms, t) for t in ts]
+    outs = ctx.selfjoin_batch([v, v], ts)
+    for got, (ref, st) in zip(outs, refs2):
+        _check_same(got, ref, st)
+
+
+def test_graph_replay_with_results_beyond_capture_capacity(ctx):
+    """When new contents produce more pairs than the captured capacity, the call
+    falls back to the exact eager path."""
+    import torch
+    n, L = 3000, 12
+    rng = np.random.default_rng(8)
+    tok = np.concatenate([np.sort(rng.choice(5000, L, replace=False)) for _ in range(n)]).astype(np.uint32)
+    s = F.Sets(np.arange(1, n + 1), np.arange(n) * L, np.full(n, L), tok, 5000)
+    v, arrs = _device_view(s)
+    ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, 0.9)
+    for _ in range(2):
+        _check_same(ctx.selfjoin_batch([v], [0.9])[0], ref, st)
+    same = np.tile(tok[:L], n)  # every record identical: n(n-1)/2 results
+    arrs[3].copy_(torch.from_numpy(same.view(np.int32)))
+    s2 = F.Sets(s.id, s.pos, s.len, same, 5000)
+    ref2, st2 = O.join(s2.pos, s2.len, s2.tokens, s2.n_terms, 0.9)
+    got = ctx.selfjoin_batch([v], [0.9])[0]
+    _check_same(got, ref2, st2)
+    assert len(got) == n * (n - 1) // 2
