@@ -315,20 +315,30 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
             const unsigned long long l0 = launch_counter();
             cudaGraph_t graph = nullptr;
             FGSS_CK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+            bool captured = true;
             try {
                 for (int i = 0; i < n; i++) join_index(c, *js[i]);
                 batched_filter_verify(c, v, opts[0].use_model != 0, &plan);
-            } catch (...) {
-                cudaStreamEndCapture(c.stream, &graph);
-                if (graph) cudaGraphDestroy(graph);
-                throw;
+            } catch (const Error& e) {
+                captured = false;  // this call's results stand; later calls run eagerly
+                if (c.verbose) fprintf(stderr, "[fgss] graph capture skipped: %s\n", e.msg.c_str());
             }
-            FGSS_CK(cudaStreamEndCapture(c.stream, &graph));
-            const cudaError_t e = cudaGraphInstantiate(&g->exec, graph, 0);
-            cudaGraphDestroy(graph);
-            if (e != cudaSuccess) fail(FGSS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            const cudaError_t ec = cudaStreamEndCapture(c.stream, &graph);
+            (void)cudaGetLastError();
+            if (captured && ec == cudaSuccess && graph) {
+                captured = cudaGraphInstantiate(&g->exec, graph, 0) == cudaSuccess;
+                (void)cudaGetLastError();
+            } else {
+                captured = false;
+            }
+            if (graph) cudaGraphDestroy(graph);
             g->launches = launch_counter() - l0;
             launch_counter() = l0;  // captured, not launched
+            if (!captured) {
+                c.release_prefix(g->ns);
+                c.bpfx.clear();
+                return;
+            }
             g->joins = std::move(js);
             g->stamp = ++c.graphs->clock;
             if (c.graphs->entries.size() >= kMaxGraphs) {

@@ -447,7 +447,9 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         } else {
             FGSS_CK(cudaMemsetAsync(J.d_nres, 0, 8, c.stream));
         }
-        join_output(c, J, keys, vals, J.d_nres, got);
+        // under a plan, the output stage is sized at capacity so the captured
+        // graph finds every buffer at the size it has now
+        join_output(c, J, keys, vals, J.d_nres, plan ? (uint64_t)J.args.res_cap : (uint64_t)got);
         J.n_res = got;
     }
 }

@@ -57,6 +57,9 @@ struct Ctx {
         if (bytes == 0) bytes = 16;
         DevBuf& b = bufs[name];
         if (b.bytes < bytes) {
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            if (stream && cudaStreamIsCapturing(stream, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+                fail(FGSS_ERR_CUDA, "buffer " + name + " would grow during a graph capture");
             if (b.p) FGSS_CK(cudaFree(b.p));
             b.p = nullptr;
             b.bytes = 0;
