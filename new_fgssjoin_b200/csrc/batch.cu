@@ -352,9 +352,11 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
     FGSS_CK(cudaMemcpyAsync(d_args, hargs, nj * sizeof(JoinArgs), cudaMemcpyHostToDevice, c.stream));
     uint32_t* counter = c.devT<uint32_t>(c.bpfx + "b.counter", 4 + nj);
     FGSS_CK(cudaMemsetAsync(counter, 0, (4 + nj) * 4, c.stream));
-    FGSS_CK(cudaEventRecord(c.ev[4], c.stream));
+    // (inside a capture the events must be external record nodes to be timed at replay)
+    const unsigned rec_flags = capture ? cudaEventRecordExternal : 0u;
+    FGSS_CK(cudaEventRecordWithFlags(c.ev[4], c.stream, rec_flags));
     if (nitems) fused_launch(c, te, d_args, d_fargs, items, (uint32_t)nitems, counter);
-    FGSS_CK(cudaEventRecord(c.ev[5], c.stream));
+    FGSS_CK(cudaEventRecordWithFlags(c.ev[5], c.stream, rec_flags));
     c.probe_timed = true;
     // heavy queries: one persistent launch per join.  Eagerly only when some
     // were queued; under a plan always, with scratch for a fixed slot count
