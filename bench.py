@@ -94,6 +94,24 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def profiled_traffic(workload):
+    """DRAM bytes (read + write) of one k_fused launch from the committed ncu
+    summary of this workload (profiles/k_fused_<workload>.md), or None."""
+    import re
+    path = os.path.join(ROOT, "profiles", "k_fused_%s.md" % workload)
+    if not os.path.exists(path):
+        return None
+    scale = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
+    tot = 0.0
+    found = 0
+    for line in open(path):
+        m = re.match(r"\| dram__bytes_(read|write)\.sum \| ([0-9.]+) (\w+) \|", line)
+        if m:
+            tot += float(m.group(2)) * scale.get(m.group(3), 1.0)
+            found += 1
+    return tot if found == 2 else None
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -291,9 +309,10 @@ def main():
                       "overflow_retries": sum(s["overflow_retries"] for s in last)},
             "e2e": {"value": ws * cands / (e2e_ms / args.steps * 1e-3), "unit": "candidates/s",
                     "ms_per_step": e2e_ms / args.steps, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "hbm", "kernel": "k_probe<FUSED>", "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-                         "alg_bytes": alg_bytes, "kernel_ms": kern_ms},
+            "roofline": {"bound": "hbm", "kernel": "k_fused", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": profiled_traffic(args.workload), "traffic_source": "profiles/k_fused_%s.md"
+                         % args.workload, "alg_bytes": alg_bytes, "kernel_ms": kern_ms},
             "gpu_launches": launches * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,

@@ -107,9 +107,10 @@ static int resident_ctas(Ctx& c) {
 int fused_resident_ctas(Ctx& c, const TuneEntry& te) {
 #define FGSS_R(NT, HL, RT) \
     if (te.threads == NT && te.hash_log2 == HL && te.regs_rt == RT) return resident_ctas<NT, HL, RT>(c);
+    FGSS_R(32, 8, 1024)
+    FGSS_R(32, 9, 1024)
     FGSS_R(64, 9, 1024)
     FGSS_R(64, 9, 768)
-    FGSS_R(64, 9, 512)
     FGSS_R(64, 10, 1024)
     FGSS_R(128, 9, 1024)
     FGSS_R(128, 10, 1024)
@@ -140,10 +141,10 @@ static void launch_fused(Ctx& c, const JoinArgs* d_args, const FusedArgs* d_farg
 
 // Launch shapes the autotuner chooses from: CTA size, slot-table log2 size,
 // resident threads per SM the register budget is sized for.
-extern const int kFusedShapes[][3] = {{64, 9, 1024},   {64, 9, 768},    {64, 9, 512},   {64, 10, 1024},
-                                      {128, 9, 1024},  {128, 10, 1024}, {128, 10, 768}, {128, 11, 768},
-                                      {256, 11, 768}};
-extern const int kNumFusedShapes = 9;
+extern const int kFusedShapes[][3] = {{32, 8, 1024},  {32, 9, 1024},  {64, 9, 1024},   {64, 9, 768},
+                                      {64, 10, 1024}, {128, 9, 1024}, {128, 10, 1024}, {128, 10, 768},
+                                      {128, 11, 768}, {256, 11, 768}};
+extern const int kNumFusedShapes = 10;
 
 void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const FusedArgs* d_fargs, const uint4* items,
                   uint32_t n_items, uint32_t* counter) {
@@ -152,9 +153,10 @@ void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const Fus
         launch_fused<NT, HL, RT>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm); \
         return;                                                                                \
     }
+    FGSS_F(32, 8, 1024)
+    FGSS_F(32, 9, 1024)
     FGSS_F(64, 9, 1024)
     FGSS_F(64, 9, 768)
-    FGSS_F(64, 9, 512)
     FGSS_F(64, 10, 1024)
     FGSS_F(128, 9, 1024)
     FGSS_F(128, 10, 1024)

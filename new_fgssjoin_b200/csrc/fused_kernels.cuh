@@ -42,12 +42,19 @@ __device__ unsigned long long g_phase_cycles[8];
 #define FGSS_PHASE(i) (void)0
 #endif
 
+// Slot word: source id (32) | query position of the last match (11) |
+// source position of the last match (11; 2047 = too large to keep) |
+// number of prefix matches (10).
+constexpr uint32_t kSmaxUnknown = 2047;
+
 // Layout: slots u64[H] | occ u16[H] | wlo,whi,clo u32[PC] | wpre u32[PC+4] | qtok u32[QC] | bm u32[BW]
 template <int HLOG>
 struct FusedLayout {
     static constexpr uint32_t H = 1u << HLOG;
     static constexpr uint32_t cap = H / 2;    // window entries per chunk
-    static constexpr uint32_t PC = H / 4 > 256 ? H / 4 : 256;  // probe tokens handled in shared memory
+    // probe tokens handled in shared memory: 256..512 (a slot's 11-bit query
+    // position and 10-bit match count rely on PC <= 512)
+    static constexpr uint32_t PC = H / 4 > 512 ? 512 : (H / 4 > 256 ? H / 4 : 256);
     static constexpr uint32_t QC = H / 2;     // query tokens staged in shared memory (longer: read from HBM)
     static constexpr uint32_t BW = 1024;      // bitmap words: 32768 bits
     static constexpr size_t off_occ = 8ull * H;
@@ -333,8 +340,9 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                     sv[u] = kEmpty;
                     if (f < L) {
                         while (wpre[j + 1] <= f) j++;
-                        sv[u] = __ldg(a.ent_s + clo[j] + (f - wpre[j]));
-                        jv[u] = j;
+                        const uint32_t k = clo[j] + (f - wpre[j]);
+                        sv[u] = __ldg(a.ent_s + k);
+                        jv[u] = (j << 11) | min((uint32_t)__ldg(a.ent_p + k), kSmaxUnknown);
                     }
                 }
 #pragma unroll
@@ -342,7 +350,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                     const uint32_t s = sv[u];
                     if (s == kEmpty) continue;
                     if (unsorted && !size_ok(a, lq, a.len[s])) continue;
-                    const uint32_t jj = jv[u];
+                    const uint32_t pos = jv[u];  // query position << 11 | source position
                     uint32_t h = hash_slot(s, hl);
                     bool done = false;
                     unsigned long long old = kEmptySlot;  // first try assumes an empty slot
@@ -351,9 +359,11 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                         unsigned long long nw;
                         if (key == s) {
                             const uint32_t lo = (uint32_t)old;
-                            nw = ((unsigned long long)s << 32) | ((((lo >> 16) + 1u) << 16) | max(lo & 0xffffu, jj));
+                            // positions of later matches are larger on both sides: keep the max
+                            const uint32_t lastpos = max(lo >> 10, pos);
+                            nw = ((unsigned long long)s << 32) | (lastpos << 10) | ((lo & 0x3ffu) + 1u);
                         } else if (key == kEmpty) {
-                            nw = ((unsigned long long)s << 32) | ((1u << 16) | jj);
+                            nw = ((unsigned long long)s << 32) | (pos << 10) | 1u;
                         } else {
                             h = (h + 1) & mask;
                             it++;
@@ -408,25 +418,32 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                     } else {
                         const unsigned long long v = slots[occ[i]];
                         s = (uint32_t)(v >> 32);
-                        c = ((uint32_t)v >> 16) & 0xffffu;
-                        const uint32_t jm = (uint32_t)v & 0xffffu;
+                        const uint32_t lo = (uint32_t)v;
+                        c = lo & 0x3ffu;
+                        const uint32_t jm = lo >> 21, smx = (lo >> 10) & 0x7ffu;
                         const uint4 sm4 = fa.meta[s];  // (pos, len, index prefix)
                         ls = sm4.y;
                         st = a.tok + sm4.x;
                         const uint4 sm = fa.smin[lq + ls];
                         xq = qsrc[jm];
                         const uint32_t A = lq - jm;
-                        const bool cand =
-                            (c + A >= sm.x) && smax_le(st, (int)ls + (int)c - (int)sm.x, c, sm4.z, xq);
-                        const bool ver =
-                            (c + A - 1 >= sm.y) && smax_le(st, (int)ls + (int)c - 1 - (int)sm.y, c, sm4.z, xq);
+                        bool cand, ver;
+                        if (smx != kSmaxUnknown) {
+                            // exact last match on both sides (filtering.cu:127-135 at the last match)
+                            cand = c + min(A, ls - smx) >= sm.x;
+                            ver = c + min(A - 1, ls - smx - 1) >= sm.y;
+                        } else {
+                            cand = (c + A >= sm.x) && smax_le(st, (int)ls + (int)c - (int)sm.x, c, sm4.z, xq);
+                            ver = (c + A - 1 >= sm.y) && smax_le(st, (int)ls + (int)c - 1 - (int)sm.y, c, sm4.z, xq);
+                        }
                         my_cand += cand;
                         if (ver) {
                             im = sm.y;
                             need = sm.z;
                             qrest = lq - jm - 1;
                             cnt = c;
-                            k = c;  // the last match sits at or after position c - 1
+                            // resume right after the last match (or at c when its position was not kept)
+                            k = smx != kSmaxUnknown ? smx + 1 : c;
                             p0 = k;
                             if (k >= ls || cnt + min(ls - k, qrest) < im) tally(c, k);
                             else have = true;
