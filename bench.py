@@ -4,15 +4,25 @@ Workload (default, "titles100k"): 100,000 synthetic title records (5-15 words,
 Zipf(1.1) over a seeded 50,000-word vocabulary, 10 % perturbed copies),
 padded lower-case 3-grams with distinct ids by ascending frequency, self-joined
 at every threshold t in {0.5, 0.6, 0.7, 0.8, 0.9}.  One step = the five joins.
-"heavy1m" is the 1M heavy-tailed-record workload at t = 0.7.
+Other workloads:
+  heavy1m    1,000,000 heavy-tailed records (lognormal word counts, 2-600 words,
+             5 % near-duplicate clusters), t = 0.7;
+  reads500k  500,000 150-base reads from a seeded 5 Mbp genome (0.5 % substitutions),
+             canonical 16-mer sets, t = 0.8;
+  batch256   256 independent joins of title records, log-uniform sizes 1,000-200,000,
+             each with its own t from {0.6, 0.7, 0.8, 0.9, 0.95}; one step = the 256
+             joins, batched in one call against 256 sequential plain calls, with the
+             per-join latency p50/p99 of both forms;
+  titles18k, heavy300k  smaller cases (the 18k-title join at t = 0.9; a profiling size).
 
 Metric: candidates per second (candidates = the reference's "# Candidates"
 counter, identical for every method) of the batched + learned form; the plain
 per-stage form is timed on the same step and reported beside it, with a check
 that both pair sets are identical.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload titles100k|heavy1m|titles18k|heavy300k]
-                 [--thresholds 0.7,0.9] [--no-model] [--no-tune] [--no-cpu-baseline]
+  python bench.py [--gpus N] [--steps K] [--warmup W]
+                  [--workload titles100k|heavy1m|reads500k|batch256|titles18k|heavy300k]
+                  [--thresholds 0.7,0.9] [--no-model] [--no-tune] [--no-cpu-baseline]
   python bench.py --impl reference ...   # the CPU restatement of the reference algorithm
 """
 import argparse
@@ -30,17 +40,57 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     "titles100k": dict(kind="titles", n=100_000, seed=2, thresholds=[0.5, 0.6, 0.7, 0.8, 0.9]),
     "heavy1m": dict(kind="heavy", n=1_000_000, seed=3, thresholds=[0.7]),
+    "reads500k": dict(kind="reads", n=500_000, seed=5, thresholds=[0.8]),
+    "batch256": dict(kind="batch", joins=256, lo=1000, hi=200_000, seed=6),
     "titles18k": dict(kind="titles", n=18_000, seed=1, thresholds=[0.9]),
     "heavy300k": dict(kind="heavy", n=300_000, seed=4, thresholds=[0.7]),  # profiling size: > L2, a few GB
 }
+GENOME_LEN = 5_000_000
 
 
 def make_text(w, seed_offset=0, n=None):
+    """One record file of a single-file workload (``n`` overrides its size; a
+    smaller read sample keeps the genome's coverage by shrinking the genome)."""
     from new_fgssjoin_b200 import datagen
     n = n or w["n"]
     if w["kind"] == "titles":
         return datagen.titles(n, seed=w["seed"] + seed_offset)
+    if w["kind"] == "reads":
+        return datagen.reads(n, seed=w["seed"] + seed_offset, genome_len=max(10_000, GENOME_LEN * n // w["n"]))
     return datagen.heavy(n, seed=w["seed"] + seed_offset)
+
+
+def _titles_job(args):
+    from new_fgssjoin_b200 import datagen
+    n, seed = args
+    return datagen.titles(int(n), seed=int(seed))
+
+
+def workload_jobs(w, seed_offset=0, n=None, only=None):
+    """-> (texts, jobs): the record files of one step and its joins as
+    (text index, threshold).  The 256-join batch draws log-uniform sizes and a
+    threshold per join (datagen.batch_sizes); its files are generated in a
+    spawned process pool before the first GPU call.  ``only``: the file
+    indices to generate (the others are None)."""
+    if w["kind"] != "batch":
+        return [make_text(w, seed_offset, n)], [(0, t) for t in w["thresholds"]]
+    from new_fgssjoin_b200 import datagen
+    sizes, ts = datagen.batch_sizes(w["joins"], w["lo"], w["hi"], seed=w["seed"] + seed_offset)
+    if n:
+        sizes = np.minimum(sizes, n)
+    keep = range(len(sizes)) if only is None else sorted(only)
+    work = [(int(sizes[i]), (w["seed"] + seed_offset) * 100_003 + i) for i in keep]
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    made = []
+    if work:
+        with cf.ProcessPoolExecutor(max_workers=max(1, min(32, os.cpu_count() or 1, len(work))),
+                                    mp_context=mp.get_context("spawn")) as ex:
+            made = list(ex.map(_titles_job, work, chunksize=2))
+    texts = [None] * len(sizes)
+    for i, t in zip(keep, made):
+        texts[i] = t
+    return texts, [(i, float(t)) for i, t in enumerate(ts)]
 
 
 def dist_env():
@@ -120,46 +170,104 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_reference(w, steps, warmup, sample_note):
-    """The reference algorithm on the host cores (oracle restatement, OpenMP)."""
+def cpu_sample(w, jobs):
+    """The bounded CPU sample of one step: every join of a single-file workload;
+    every 8th join of the 256-join batch (32 joins, about 1/8 of its records)."""
+    if w["kind"] == "batch":
+        return [j for k, j in enumerate(jobs) if k % 8 == 0]
+    return list(jobs)
+
+
+def oracle_sets(w, texts, sample):
+    """Memory-order records of the sampled files, tokenized by the oracle."""
     from oracle import oracle as O
-    text = make_text(w)
-    ids, lens, tok, loc, nt = O.tokenize(text, **tok_opts(w))
-    mid, mpos, mlen, mtok = O.file_to_memory(ids, lens, tok)
+    mem = {}
+    for ti, _ in sample:
+        if ti not in mem:
+            ids, lens, tok, loc, nt = O.tokenize(texts[ti], **tok_opts(w))
+            _, mpos, mlen, mtok = O.file_to_memory(ids, lens, tok)
+            mem[ti] = (mpos, mlen, mtok, nt)
+    return mem
+
+
+def cpu_reference(w, jobs, mem, steps, warmup):
+    """The reference algorithm on the host cores (oracle restatement, OpenMP)
+    over the bounded sample of one step; ``mem`` maps a file index to its
+    memory-order (pos, len, tokens, n_terms).
+    -> (candidates/s, ms per sample, threads, note)."""
+    from oracle import oracle as O
+    sample = cpu_sample(w, jobs)
     threads = O.lib().orc_num_threads()
     times, cands = [], []
     for it in range(warmup + steps):
         t0 = time.perf_counter()
         c = 0
-        for t in w["thresholds"]:
+        for ti, t in sample:
+            mpos, mlen, mtok, nt = mem[ti]
             _, st = O.join(mpos, mlen, mtok, nt, t, threads=threads)
             c += st["candidates"]
         dt = time.perf_counter() - t0
         if it >= warmup:
             times.append(dt)
             cands.append(c)
-    return float(np.sum(cands) / np.sum(times)), float(np.mean(times) * 1000.0), threads
+    recs = sum(len(mem[ti][1]) for ti in {ti for ti, _ in sample})
+    note = ("%d of %d joins (%d records), oracle restatement, OpenMP, %d threads"
+            % (len(sample), len(jobs), recs, threads))
+    return float(np.sum(cands) / np.sum(times)), float(np.mean(times) * 1000.0), threads, note
 
 
 def tok_opts(w):
     from new_fgssjoin_b200 import datagen
-    return dict(datagen.TITLE_TOK)
+    return dict(datagen.READ_TOK if w["kind"] == "reads" else datagen.TITLE_TOK)
+
+
+METRIC = "self-join candidates/s (batched+learned vs plain GPU, identical pair set)"
 
 
 def run_reference(args, w):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    v, ms, threads = cpu_reference(w, args.steps, args.warmup, "")
-    sample = "full step: %d records x thresholds %s (oracle restatement, OpenMP)" % (w["n"], w["thresholds"])
-    line = {"metric": "self-join candidates/s (batched+learned vs plain GPU, identical pair set)",
-            "impl": "reference", "value": v, "unit": "candidates/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator, see bench.py docstring)",
-            "config": {"workload": args.workload, "records": w["n"], "thresholds": w["thresholds"]},
-            "cpu_baseline": {"value": v, "unit": "candidates/s", "cores": threads, "kind": "port", "sample": sample},
+    _, jobs = workload_jobs(w, only=())
+    sample = cpu_sample(w, jobs)
+    texts, _ = workload_jobs(w, only={ti for ti, _ in sample})
+    v, ms, threads, note = cpu_reference(w, jobs, oracle_sets(w, texts, sample), args.steps, args.warmup)
+    line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "candidates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded generator, see bench.py docstring)",
+            "config": {"workload": args.workload, "joins_per_step": len(jobs),
+                       "thresholds": sorted({t for _, t in jobs})},
+            "cpu_baseline": {"value": v, "unit": "candidates/s", "cores": threads, "kind": "port", "sample": note},
             "e2e": {"value": v, "unit": "candidates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def model_report(used, loss, first, timed, n_joins):
+    """The learned model's error against the exact counts of the same joins, and
+    how often its presized result buffers overflowed (an exact re-run each)."""
+    rep = {"used": used, "train_loss": loss}
+    if not used:
+        return rep
+
+    def err(key, pkey):
+        p = np.array([s[pkey] for s in first], np.float64)
+        a = np.array([s[key] for s in first], np.float64)
+        rel = np.abs(p - a) / np.maximum(a, 1.0)
+        return {"predicted": float(p.sum()), "actual": float(a.sum()),
+                "total_rel_err": float(abs(p.sum() - a.sum()) / max(a.sum(), 1.0)),
+                "per_join_rel_err_p50": float(np.median(rel)), "per_join_rel_err_p90": float(np.percentile(rel, 90))}
+    rep["candidates"] = err("candidates", "predicted_candidates")
+    rep["results"] = err("results", "predicted_results")
+    rep["overflow_first_call"] = "%d of %d joins" % (sum(s["overflow_retries"] for s in first), n_joins)
+    rep["overflow_timed_steps"] = "%d of %d joins" % (sum(s["overflow_retries"] for st in timed for s in st),
+                                                       n_joins * len(timed))
+    return rep
+
+
+def _pct(xs):
+    xs = np.asarray(xs, dtype=np.float64)
+    return {"p50": float(np.percentile(xs, 50)), "p99": float(np.percentile(xs, 99)), "max": float(xs.max())}
 
 
 def main():
@@ -175,14 +283,24 @@ def main():
     ap.add_argument("--thresholds", type=str, default=None, help="comma-separated, overrides the workload's")
     args = ap.parse_args()
     w = dict(WORKLOADS[args.workload])
-    if args.thresholds:
+    if args.thresholds and w["kind"] != "batch":
         w["thresholds"] = [float(x) for x in args.thresholds.split(",")]
     if args.impl == "reference":
         return run_reference(args, w)
 
+    ws, rank, local = dist_env()
+    # record files (untimed) are generated before the first GPU call
+    texts, jobs = workload_jobs(w, seed_offset=rank * 1000)
+    train_texts = []
+    if not args.no_model:
+        # a 30k-record sample of a single-file workload; 8 joins of another batch draw
+        train_texts, _ = workload_jobs(w, seed_offset=7919 + rank, n=None if w["kind"] == "batch" else 30000,
+                                       only=range(8))
+        train_texts = [x for x in train_texts if x is not None]
+
     import torch
     import new_fgssjoin_b200 as F
-    ws, rank, local = dist_env()
+    from new_fgssjoin_b200.binding import _View
     torch.cuda.set_device(local)
     if ws > 1:
         import torch.distributed as dist
@@ -191,80 +309,135 @@ def main():
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
     ctx = F.Context(device=local, stream=stream.cuda_stream)
+    to = tok_opts(w)
 
-    # ---- inputs (untimed): text -> GPU tokenizer -> device-resident sets
-    text = make_text(w, seed_offset=rank * 1000)
-    sets = ctx.tokenize(text, **tok_opts(w))
-    d_arrays = [torch.from_numpy(a.view(np.int32)).to(dev) for a in (sets.id, sets.pos, sets.len, sets.tokens)]
+    # ---- inputs (untimed): text -> GPU tokenizer -> device-resident sets + pinned host copies
+    sets, d_arrays, host_sets = [], [], []
+    for text in texts:
+        s = ctx.tokenize(text, **to)
+        sets.append(s)
+        d_arrays.append([torch.from_numpy(a.view(np.int32)).to(dev) for a in (s.id, s.pos, s.len, s.tokens)])
+        pinned = [torch.from_numpy(a.view(np.int32)).pin_memory() for a in (s.id, s.pos, s.len, s.tokens)]
+        host_sets.append(F.Sets(*(p.numpy().view(np.uint32) for p in pinned), n_terms=s.n_terms))
+    del texts
 
-    def dev_view():
-        from new_fgssjoin_b200.binding import _View
+    def dev_view(ti):
         v = _View()
-        v.id, v.pos, v.len, v.tokens = [t.data_ptr() for t in d_arrays]
-        v.n_sets, v.n_tokens, v.n_terms, v.on_device = sets.n_sets, sets.n_tokens, sets.n_terms, 1
+        v.id, v.pos, v.len, v.tokens = [t.data_ptr() for t in d_arrays[ti]]
+        s = sets[ti]
+        v.n_sets, v.n_tokens, v.n_terms, v.on_device = s.n_sets, s.n_tokens, s.n_terms, 1
         return v
 
-    ts = w["thresholds"]
-    # pinned host copies for the end-to-end leg
-    pinned = [torch.from_numpy(a.view(np.int32)).pin_memory() for a in (sets.id, sets.pos, sets.len, sets.tokens)]
-    host_sets = F.Sets(*(p.numpy().view(np.uint32) for p in pinned), n_terms=sets.n_terms)
+    def host_view(ti):
+        return host_sets[ti].view()
+
+    ts = [t for _, t in jobs]
+    t_list = sorted(set(ts))
 
     # ---- learned cost model: trained (untimed) on a different sample of the workload
     use_model = not args.no_model
     model_loss = None
     if use_model:
-        train_text = make_text(w, seed_offset=7919 + rank, n=min(w["n"], 30000))
-        train_sets = ctx.tokenize(train_text, **tok_opts(w))
-        model_loss = ctx.model_train([train_sets] * len(ts), ts, epochs=300, lr=0.01, seed=1)
+        tr = [ctx.tokenize(x, **to) for x in train_texts]
+        k_n = max(len(tr), len(t_list))
+        model_loss = ctx.model_train([tr[k % len(tr)] for k in range(k_n)],
+                                     [t_list[k % len(t_list)] for k in range(k_n)], epochs=300, lr=0.01, seed=1)
+        del tr
 
-    # autotuner (untimed): fastest fused-kernel shape per threshold, cached in the context
+    # autotuner (untimed): fastest fused-kernel shape per threshold on its largest join, cached in the context
     tuned = {}
     if not args.no_tune:
-        for t in ts:
-            tuned[str(t)] = ctx.autotune(dev_view(), t, reps=1)
+        for t in t_list:
+            ti = max((j for j in jobs if j[1] == t), key=lambda j: sets[j[0]].n_tokens)[0]
+            tuned[str(t)] = ctx.autotune(dev_view(ti), t, reps=1)
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
 
-    def step(method, view_fn, model):
-        return ctx.selfjoin_batch([view_fn()] * len(ts), ts, method=method, use_model=model)
+    def step_batched(view_fn):
+        return ctx.selfjoin_batch([view_fn(ti) for ti, _ in jobs], ts, method="batched", use_model=use_model)
 
-    def timed(method, view_fn, model, k, wu):
-        for _ in range(wu):
-            step(method, view_fn, model)
+    def step_plain(view_fn, per_join_ms=None):
+        """The plain form: the joins one after another, one call each."""
+        outs = []
+        for ti, t in jobs:
+            if per_join_ms is not None:
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+            outs += ctx.selfjoin_batch([view_fn(ti)], [t], method="plain")
+            if per_join_ms is not None:
+                b.record(stream)
+                b.synchronize()
+                per_join_ms.append(a.elapsed_time(b))
+        return outs
+
+    def barrier():
         torch.cuda.synchronize(dev)
         if ws > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize(dev)
-        tot_ms, outs = 0.0, None
-        stats = []
+
+    first_stats = []
+
+    def timed(fn, k, wu):
+        for i in range(wu):
+            outs = fn()
+            if i == 0:
+                first_stats.append([o.stats for o in outs])
+        barrier()
+        tot_ms, outs, stats = 0.0, None, []
         for _ in range(k):
             flush.fill_(1.0)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            outs = step(method, view_fn, model)
+            outs = fn()
             e1.record(stream)
             e1.synchronize()
             tot_ms += e0.elapsed_time(e1)
             stats.append([o.stats for o in outs])
-        torch.cuda.synchronize(dev)
-        if ws > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize(dev)
+        barrier()
         return tot_ms, outs, stats
 
     clocks = Clocks(local)
-    bat_ms, bat_out, bat_stats = timed("batched", dev_view, use_model, args.steps, args.warmup)
+    bat_ms, bat_out, bat_stats = timed(lambda: step_batched(dev_view), args.steps, args.warmup)
     clk = clocks.stop()
-    plain_ms, plain_out, _ = timed("plain", dev_view, False, max(1, args.steps // 2), 1)
     plain_steps = max(1, args.steps // 2)
+    plain_join_ms = []
+    plain_ms, plain_out, _ = timed(lambda: step_plain(dev_view, plain_join_ms), plain_steps, 1)
     same = all(np.array_equal(a.q, b.q) and np.array_equal(a.s, b.s) and np.array_equal(a.overlap, b.overlap)
                for a, b in zip(bat_out, plain_out))
     cands = sum(o.stats["candidates"] for o in bat_out)
     # e2e: host (pinned) inputs, H2D + join + D2H of the pairs inside the timed region
-    e2e_ms, e2e_out, _ = timed("batched", host_sets.view, use_model, args.steps, 1)
-    h2d = sum(a.nbytes for a in (sets.id, sets.pos, sets.len, sets.tokens)) * len(ts)
+    e2e_ms, e2e_out, _ = timed(lambda: step_batched(host_view), args.steps, 1)
+    h2d = sum(sum(a.nbytes for a in (sets[ti].id, sets[ti].pos, sets[ti].len, sets[ti].tokens)) for ti, _ in jobs)
     d2h = sum(len(o) * 24 for o in e2e_out)
+    same_e2e = all(np.array_equal(a.q, b.q) and np.array_equal(a.s, b.s) for a, b in zip(e2e_out, plain_out))
+
+    # per-join latency (the 256-join batch): every join of the batch finishes when the batched call
+    # returns; the plain joins finish one after another.  "alone": each join run by itself.
+    per_join = None
+    if w["kind"] == "batch":
+        nj = len(jobs)
+        pj = np.asarray(plain_join_ms[-nj:], dtype=np.float64)
+        alone_b = []
+        for ti, t in jobs:
+            ctx.selfjoin_batch([dev_view(ti)], [t], method="batched", use_model=use_model)  # records + captures
+            flush.fill_(1.0)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ctx.selfjoin_batch([dev_view(ti)], [t], method="batched", use_model=use_model)
+            b.record(stream)
+            b.synchronize()
+            alone_b.append(a.elapsed_time(b))
+        per_step = bat_ms / args.steps
+        per_join = {"unit": "ms",
+                    "batched_completion": _pct([per_step] * nj),
+                    "plain_sequential_completion": _pct(np.cumsum(pj)),
+                    "batched_alone": _pct(alone_b),
+                    "plain_alone": _pct(pj),
+                    "sizes_records": _pct([sets[ti].n_sets for ti, _ in jobs])}
 
     # max over ranks
     vals = torch.tensor([bat_ms, plain_ms, e2e_ms], dtype=torch.float64, device=dev)
@@ -272,7 +445,7 @@ def main():
         torch.distributed.all_reduce(vals, op=torch.distributed.ReduceOp.MAX)
     bat_ms, plain_ms, e2e_ms = vals.tolist()
 
-    # roofline of the fused filter+verify kernel (per launch = one step's five joins)
+    # roofline of the fused filter+verify kernel (one launch per step covers every join of the step)
     last = bat_stats[-1]
     kern_ms = float(np.mean([s[0]["ms_probe"] for s in bat_stats]))
     P = sum(s["probe_tokens"] for s in last)
@@ -286,27 +459,29 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        v, ms, threads = cpu_reference(w, 1, 0, "")
-        cpu = {"value": v, "unit": "candidates/s", "cores": threads, "kind": "port",
-               "sample": "one full step (%d records x %d thresholds), oracle restatement, OpenMP" % (w["n"], len(ts))}
+        # the same records the GPU joined (the GPU tokenizer's output equals the oracle's)
+        mem = {ti: (sets[ti].pos, sets[ti].len, sets[ti].tokens, sets[ti].n_terms) for ti, _ in cpu_sample(w, jobs)}
+        v, ms, threads, note = cpu_reference(w, jobs, mem, 1, 0)
+        cpu = {"value": v, "unit": "candidates/s", "cores": threads, "kind": "port", "sample": note}
 
     if rank == 0:
         per_step = bat_ms / args.steps
+        uniq = sorted({ti for ti, _ in jobs})
         line = {
-            "metric": "self-join candidates/s (batched+learned vs plain GPU, identical pair set)",
+            "metric": METRIC,
             "value": ws * cands / (per_step * 1e-3), "unit": "candidates/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator, see bench.py docstring)",
-            "config": {"workload": args.workload, "records": sets.n_sets, "tokens": sets.n_tokens,
-                       "thresholds": ts, "joins_per_step": len(ts), "l2": "flushed between steps (256 MB write)",
-                       "parallelism": "replicas x%d" % ws},
+            "config": {"workload": args.workload, "records": sum(sets[ti].n_sets for ti in uniq),
+                       "tokens": sum(sets[ti].n_tokens for ti in uniq),
+                       "thresholds": t_list, "joins_per_step": len(jobs),
+                       "l2": "flushed between steps (256 MB write)", "parallelism": "replicas x%d" % ws},
             "plain_ms_per_step": plain_ms / plain_steps,
             "speedup_vs_plain": (plain_ms / plain_steps) / per_step,
-            "pair_sets_identical": bool(same),
+            "pair_sets_identical": bool(same and same_e2e),
             "candidates_per_step": cands, "results_per_step": R,
             "autotune": {t: "%dx%d/rt%d" % (v["threads"], v["hash_log2"], v["regs_rt"]) for t, v in tuned.items()},
-            "model": {"used": use_model, "train_loss": model_loss,
-                      "overflow_retries": sum(s["overflow_retries"] for s in last)},
+            "model": model_report(use_model, model_loss, first_stats[0], bat_stats, len(jobs)),
             "e2e": {"value": ws * cands / (e2e_ms / args.steps * 1e-3), "unit": "candidates/s",
                     "ms_per_step": e2e_ms / args.steps, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "kernel": "k_fused", "achieved": achieved, "peak": peak,
@@ -317,6 +492,8 @@ def main():
             "clocks": clk,
             "cpu_baseline": cpu,
         }
+        if per_join:
+            line["per_join_latency"] = per_join
         print(json.dumps(line), flush=True)
     ctx.close()
     if ws > 1:

@@ -173,6 +173,8 @@ typedef struct fgss_stats {
     float ms_probe;           /* batched method: the fused filter+verify kernel alone */
     uint64_t merged_tokens;   /* source tokens the fused kernel's merges read */
     uint64_t launches;        /* kernels launched by the call */
+    uint64_t predicted_candidates; /* batched method with use_model: the learned model's estimates */
+    uint64_t predicted_results;    /* of candidates and results (0 otherwise; the exact counts judge them) */
 } fgss_stats;
 
 typedef struct fgss_pairs {

@@ -61,7 +61,8 @@ class _Stats(ctypes.Structure):
                 ("heavy_queries", ctypes.c_uint64), ("overflow_retries", ctypes.c_uint32),
                 ("ms_total", ctypes.c_float), ("ms_index", ctypes.c_float), ("ms_filter", ctypes.c_float),
                 ("ms_verify", ctypes.c_float), ("ms_output", ctypes.c_float), ("ms_probe", ctypes.c_float),
-                ("merged_tokens", ctypes.c_uint64), ("launches", ctypes.c_uint64)]
+                ("merged_tokens", ctypes.c_uint64), ("launches", ctypes.c_uint64),
+                ("predicted_candidates", ctypes.c_uint64), ("predicted_results", ctypes.c_uint64)]
 
 
 class _Pairs(ctypes.Structure):
@@ -353,11 +354,13 @@ class Context:
         _check(self._L, self._ctx, rc)
         return self._collect(p, st, want_candidates)
 
-    def selfjoin_batch(self, sets_list, thresholds, method="batched", bounds="reference", use_model=False):
+    def selfjoin_batch(self, sets_list, thresholds, method="batched", bounds="reference", use_model=False,
+                       result_capacity=0):
         """Many independent self-joins in one call (one persistent launch per stage)."""
         n = len(sets_list)
         views = (_View * n)(*[s.view() if isinstance(s, Sets) else s for s in sets_list])
-        opts = (_JoinOpts * n)(*[self._opts(t, method, bounds, False, use_model) for t in thresholds])
+        opts = (_JoinOpts * n)(*[self._opts(t, method, bounds, False, use_model, result_capacity=result_capacity)
+                                 for t in thresholds])
         outs = (_Pairs * n)()
         sts = (_Stats * n)()
         rc = self._L.fgss_selfjoin_batch(self._ctx, views, opts, n, outs, sts)

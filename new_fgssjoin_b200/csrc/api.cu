@@ -63,6 +63,8 @@ void fill_stats(const JoinState& J, fgss_stats* st) {
     st->heavy_queries = J.stats_host[SS_HEAVY];
     st->overflow_retries = J.overflow_retries;
     st->merged_tokens = J.stats_host[SS_MERGED];
+    st->predicted_candidates = J.pred_candidates;
+    st->predicted_results = J.pred_results;
 }
 
 void export_pairs(Ctx& c, JoinState& J, const fgss_join_opts& o, fgss_pairs* out) {
@@ -156,7 +158,8 @@ void report_stats(Ctx& c, std::vector<JoinState*>& js, fgss_stats* stats, unsign
 // presized buffer overflowed.
 namespace fgss {
 struct GraphEntry {
-    cudaGraphExec_t exec = nullptr;
+    cudaGraphExec_t exec = nullptr;   // null: not captured (yet); calls run eagerly in ns
+    int failed_captures = 0;
     std::string ns;
     std::vector<std::unique_ptr<JoinState>> joins;
     unsigned long long launches = 0;  // kernels inside the graph
@@ -172,6 +175,7 @@ struct GraphCache {
 namespace {
 
 constexpr size_t kMaxGraphs = 4;
+constexpr int kMaxCaptureTries = 2;  // an entry whose capture failed this often stays eager
 
 void drop_graph(Ctx& c, std::unique_ptr<GraphEntry>& g) {
     if (g->exec) cudaGraphExecDestroy(g->exec);
@@ -218,9 +222,11 @@ bool replay_graph(Ctx& c, GraphEntry& g, const fgss_sets_view* sets, const fgss_
         // validation and fresh counters; the captured arguments (result buffers
         // and capacities) stay as they were recorded
         const JoinArgs saved = g.joins[i]->args;
-        join_setup(c, *g.joins[i], sets[i], opts[i], i);
+        join_setup(c, *g.joins[i], sets[i], opts[i], i, false);
         g.joins[i]->args = saved;
     }
+    c.sync();
+    for (int i = 0; i < n; i++) join_check_input(c, *g.joins[i]);
     FGSS_CK(cudaEventRecord(c.ev[1], c.stream));
     FGSS_CK(cudaGraphLaunch(g.exec, c.stream));
     launch_counter() += g.launches;
@@ -258,28 +264,33 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
     bool graphable = batched && !c.tune_force && c.graphs;
     for (int i = 0; i < n; i++) graphable &= sets[i].on_device != 0 && !opts[i].no_graph;
     std::string gkey;
+    std::unique_ptr<GraphEntry> g;
     if (graphable) {
         gkey = graph_key(sets, opts, n);
         auto it = c.graphs->entries.find(gkey);
         if (it != c.graphs->entries.end()) {
             it->second->stamp = ++c.graphs->clock;
-            bool ok = false;
-            try {
-                ok = replay_graph(c, *it->second, sets, opts, n, outs, stats);
-            } catch (...) {
-                c.bpfx.clear();
-                throw;
+            if (it->second->exec) {
+                bool ok = false;
+                try {
+                    ok = replay_graph(c, *it->second, sets, opts, n, outs, stats);
+                } catch (...) {
+                    c.bpfx.clear();
+                    throw;
+                }
+                if (ok) return;
+                for (int i = 0; i < n; i++) fgss_pairs_free(&outs[i]);
+                // its plan no longer fits the data: record a new one in the same buffers
+                cudaGraphExecDestroy(it->second->exec);
+                it->second->exec = nullptr;
             }
-            if (ok) return;
-            for (int i = 0; i < n; i++) fgss_pairs_free(&outs[i]);
-            drop_graph(c, it->second);  // its plan no longer fits the data
+            g = std::move(it->second);
             c.graphs->entries.erase(it);
         }
-    }
-    std::unique_ptr<GraphEntry> g;
-    if (graphable) {
-        g.reset(new GraphEntry());
-        g->ns = "g" + std::to_string(c.graphs->next_id++) + ".";
+        if (!g) {
+            g.reset(new GraphEntry());
+            g->ns = "g" + std::to_string(c.graphs->next_id++) + ".";
+        }
         c.bpfx = g->ns;
     }
     std::vector<std::unique_ptr<JoinState>> js(n);
@@ -292,9 +303,11 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
         for (int i = 0; i < n; i++) {
             js[i].reset(new JoinState());
             if (g) js[i]->ns = g->ns;
-            join_setup(c, *js[i], sets[i], opts[i], i);
-            join_index(c, *js[i]);
+            join_setup(c, *js[i], sets[i], opts[i], i, false);
         }
+        c.sync();  // one wait for the whole batch's input validation
+        for (int i = 0; i < n; i++) join_check_input(c, *js[i]);
+        for (int i = 0; i < n; i++) join_index(c, *js[i]);
         FGSS_CK(cudaEventRecord(ev[1], c.stream));
         std::vector<JoinState*> v;
         for (int i = 0; i < n; i++) v.push_back(js[i].get());
@@ -309,7 +322,7 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
             export_pairs(c, *js[i], opts[i], &outs[i]);
         }
         report_stats(c, v, stats, launch_counter() - launches0, n);
-        if (g && plan.valid) {
+        if (g && plan.valid && g->failed_captures < kMaxCaptureTries) {
             // capture the same batch (index build included) for later calls
             plan.capture = true;
             const unsigned long long l0 = launch_counter();
@@ -334,12 +347,14 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
             if (graph) cudaGraphDestroy(graph);
             g->launches = launch_counter() - l0;
             launch_counter() = l0;  // captured, not launched
-            if (!captured) {
-                c.release_prefix(g->ns);
-                c.bpfx.clear();
-                return;
+            if (captured) {
+                g->joins = std::move(js);
+            } else {
+                g->failed_captures++;  // later calls run eagerly in the same buffers
             }
-            g->joins = std::move(js);
+        }
+        if (g) {
+            // keep the entry (and its buffers) for the next call with these inputs
             g->stamp = ++c.graphs->clock;
             if (c.graphs->entries.size() >= kMaxGraphs) {
                 auto oldest = c.graphs->entries.begin();
@@ -349,8 +364,6 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
                 c.graphs->entries.erase(oldest);
             }
             c.graphs->entries[gkey] = std::move(g);
-        } else if (g) {
-            c.release_prefix(g->ns);
         }
     } catch (...) {
         c.bpfx.clear();

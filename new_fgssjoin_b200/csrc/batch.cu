@@ -203,9 +203,10 @@ __global__ void k_clear_filter_state(uint32_t* status, unsigned long long* stats
 void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_model, BatchPlan* plan) {
     const size_t nj = joins.size();
     const bool capture = plan && plan->capture;
-    uint64_t* d_tot = c.devT<uint64_t>(c.bpfx + "b.tot", nj * 2 + 2);
+    // d_tot: [0, nj) cost totals, [nj, 2nj) predicted results, [2nj, 3nj) predicted candidates
+    uint64_t* d_tot = c.devT<uint64_t>(c.bpfx + "b.tot", nj * 3 + 2);
     std::vector<uint64_t*> pre(nj);
-    FGSS_CK(cudaMemsetAsync(d_tot, 0, (nj * 2 + 2) * 8, c.stream));
+    FGSS_CK(cudaMemsetAsync(d_tot, 0, (nj * 3 + 2) * 8, c.stream));
     FusedArgs* hf = c.pinnedT<FusedArgs>(c.bpfx + "b.hf", nj);
     TuneEntry te;
     if (capture) {
@@ -258,7 +259,7 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         if (model) {
             k_features<<<grid_for(n * 32, 256, c.num_sms * 32), 256, 0, c.stream>>>(J.args, J.t, feat, fcost);
             FGSS_LAUNCH_CK();
-            model_predict(c, feat, n, pred, &d_tot[nj + i]);
+            model_predict(c, feat, n, pred, &d_tot[nj + i], &d_tot[2 * nj + i]);
         }
         k_cost<<<grid_for(n, 256, c.num_sms * 8), 256, 0, c.stream>>>(wtot, J.in.len, model ? pred : nullptr,
                                                                        (uint32_t)n, J.args.q_lo, J.args.q_hi, cost);
@@ -269,13 +270,18 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
     FGSS_CK(cudaMemcpyAsync(d_fargs, hf, nj * sizeof(FusedArgs), cudaMemcpyHostToDevice, c.stream));
     std::vector<uint32_t> K(nj, 0);
     uint64_t nitems = 0;
-    std::vector<uint64_t> htot(2 * nj + 2, 0);
+    std::vector<uint64_t> htot(3 * nj + 2, 0);
     if (capture) {
         K = plan->K;
         nitems = plan->nitems;
     } else {
-        FGSS_CK(cudaMemcpyAsync(htot.data(), d_tot, (2 * nj + 2) * 8, cudaMemcpyDeviceToHost, c.stream));
+        FGSS_CK(cudaMemcpyAsync(htot.data(), d_tot, (3 * nj + 2) * 8, cudaMemcpyDeviceToHost, c.stream));
         c.sync();
+        for (size_t i = 0; i < nj; i++) {
+            if (!(use_model && c.model && !joins[i]->res_cap_hint)) continue;
+            joins[i]->pred_results = htot[nj + i];
+            joins[i]->pred_candidates = htot[2 * nj + i];
+        }
         uint64_t grand = 0;
         for (size_t i = 0; i < nj; i++) grand += htot[i];
         // ~32 items per resident CTA over the whole batch, split by cost share and
@@ -336,7 +342,8 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
             } else if (J.res_cap_user) {
                 cap = J.res_cap_user;
             } else if (use_model && c.model) {
-                cap = (uint64_t)((double)htot[nj + i] * 1.5) + 4096;  // predicted results x 1.5 + slack
+                // predicted results x 1.5 + slack, or the size this slot needed last time if larger
+                cap = std::max<uint64_t>((uint64_t)((double)htot[nj + i] * 1.5) + 4096, last);
             } else {
                 cap = std::max<uint64_t>(n + 4096, last);
             }
@@ -422,19 +429,25 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
     for (size_t i = 0; i < nj; i++)
         FGSS_CK(cudaMemcpyAsync(hbuf + 2 * i, joins[i]->status + 3, 4, cudaMemcpyDeviceToHost, c.stream));
     c.sync();
+    const std::vector<uint32_t> gots = [&] {
+        std::vector<uint32_t> g(nj);
+        for (size_t i = 0; i < nj; i++) g[i] = hbuf[2 * i];
+        return g;
+    }();
     for (size_t i = 0; i < nj; i++) {
         JoinState& J = *joins[i];
-        const uint32_t got = hbuf[2 * i];
+        const uint32_t got = gots[i];
         if (got > J.args.res_cap) {
             // The learned (or remembered) capacity was too small: the kernel kept
-            // counting, so re-run this join alone with the exact size.
+            // counting, so re-run this join alone with the exact size.  A plan
+            // keeps that exact size for the captured batch.
             J.res_cap_hint = got;
             J.overflow_retries++;
             k_clear_filter_state<<<1, 32, 0, c.stream>>>(J.status, J.stats);
             FGSS_LAUNCH_CK();
             std::vector<JoinState*> one{&J};
             batched_filter_verify(c, one, false, nullptr);
-            if (plan) plan->valid = false;  // a batch that overflowed is not captured
+            if (plan) plan->res_cap[i] = J.args.res_cap;
             continue;
         }
         if (plan) plan->res_cap[i] = J.args.res_cap;

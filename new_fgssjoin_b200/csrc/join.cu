@@ -79,7 +79,7 @@ DevBounds device_bounds(Ctx& c, float t, int mode) {
     return d;
 }
 
-void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_opts& o, int slot) {
+void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_opts& o, int slot, bool check) {
     J.slot = slot;
     J.t = o.threshold;
     J.res_cap_user = o.result_capacity;
@@ -158,10 +158,17 @@ void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_o
     // no kernel reads tokens through caller offsets before they are validated
     uint32_t* h = c.pinnedT<uint32_t>(J.pfx("h.prep"), 4);
     FGSS_CK(cudaMemcpyAsync(h, J.status, 4, cudaMemcpyDeviceToHost, c.stream));
+    if (!check) return;
     c.sync();
-    if (h[0] & ST_BAD_OFFSETS) fail(FGSS_ERR_FORMAT, "a record's pos + len exceeds n_tokens");
-    if (h[0] & ST_TOO_LONG) fail(FGSS_ERR_UNSUPPORTED, "a record has more than 65535 tokens");
-    if (h[0] & ST_BAD_TOKENS)
+    join_check_input(c, J);
+}
+
+void join_check_input(Ctx& c, JoinState& J) {
+    if (J.in.n_sets == 0) return;
+    const uint32_t st = c.pinnedT<uint32_t>(J.pfx("h.prep"), 4)[0];
+    if (st & ST_BAD_OFFSETS) fail(FGSS_ERR_FORMAT, "a record's pos + len exceeds n_tokens");
+    if (st & ST_TOO_LONG) fail(FGSS_ERR_UNSUPPORTED, "a record has more than 65535 tokens");
+    if (st & ST_BAD_TOKENS)
         fail(FGSS_ERR_FORMAT, "tokens must be strictly ascending inside each record and below n_terms");
 }
 

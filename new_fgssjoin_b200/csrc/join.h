@@ -54,12 +54,18 @@ struct JoinState {
     uint32_t status_host = 0;
     unsigned long long stats_host[SS_N] = {};
     std::vector<uint32_t> cand_host;  // (q, s, partial) triples when requested
+    uint64_t pred_results = 0;        // the learned model's estimates (batched method, 0 without it)
+    uint64_t pred_candidates = 0;
     std::string ns;                   // buffer-name namespace ("" or a captured graph's own "g<id>.")
     std::string pfx(const char* name) const { return ns + "j" + std::to_string(slot) + "." + name; }
 };
 
 // Stage drivers (join.cu)
-void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_opts& o, int slot);
+// Queues the input validation and the per-record counts of one join.  With
+// check=false the caller synchronizes the stream once for a whole batch and
+// then calls join_check_input for every join before any kernel reads tokens.
+void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_opts& o, int slot, bool check = true);
+void join_check_input(Ctx& c, JoinState& J);
 void join_index(Ctx& c, JoinState& J);
 void join_plain_filter_verify(Ctx& c, JoinState& J, bool want_cand);
 void join_features(Ctx& c, JoinState& J, float* d_feat);
@@ -70,7 +76,7 @@ void join_output(Ctx& c, JoinState& J, uint64_t* keys, uint32_t* vals, const uin
 // same batch is captured into a CUDA graph (batch.cu).
 struct BatchPlan {
     bool capture = false;             // issue device work only, with these decisions
-    bool valid = true;                // false: the run overflowed; do not capture it
+    bool valid = true;                // false: do not capture this run
     TuneEntry te;
     std::vector<uint32_t> K;          // work items per join
     uint64_t nitems = 0;

@@ -132,12 +132,12 @@ __global__ void k_zero(float* p, int n) {
 // Predicted candidates per query and the sum of predicted results (rounded up).
 __global__ void __launch_bounds__(256) k_mlp_predict(const float* __restrict__ feat, uint64_t n,
                                                      const float* __restrict__ Pg, uint32_t* __restrict__ pred,
-                                                     unsigned long long* res_sum) {
+                                                     unsigned long long* res_sum, unsigned long long* cand_sum) {
     __shared__ float P[kParamsAll];
     for (int i = threadIdx.x; i < kParamsAll; i += blockDim.x) P[i] = Pg[i];
     __syncthreads();
     const float calib = P[kParams + 1] > 0.f ? P[kParams + 1] : 1.f;
-    unsigned long long rs = 0;
+    unsigned long long rs = 0, cs = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         float x[kFeatM], hpre[kHidden], o[kOut];
 #pragma unroll
@@ -146,10 +146,15 @@ __global__ void __launch_bounds__(256) k_mlp_predict(const float* __restrict__ f
         float lc = fminf(fmaxf(o[0] * kOutScale, 0.f), 30.f);
         float lr = fminf(fmaxf(o[1] * kOutScale, 0.f), 30.f);
         pred[i] = (uint32_t)fminf(expm1f(lc), 1.0e9f);
+        cs += pred[i];
         rs += (unsigned long long)ceilf(expm1f(lr) * calib);
     }
     rs = warp_sum(rs);
     if (lane_id() == 0 && rs) atomicAdd(res_sum, rs);
+    if (cand_sum) {
+        cs = warp_sum(cs);
+        if (lane_id() == 0 && cs) atomicAdd(cand_sum, cs);
+    }
 }
 
 __global__ void k_sum_cost(const uint32_t* __restrict__ c, uint64_t n, unsigned long long* out) {
@@ -167,10 +172,10 @@ void model_sum_cost(Ctx& c, const uint32_t* cost, uint64_t n, uint64_t* out) {
     FGSS_LAUNCH_CK();
 }
 
-void model_predict(Ctx& c, const float* feat, uint64_t n, uint32_t* pred, uint64_t* res_sum) {
+void model_predict(Ctx& c, const float* feat, uint64_t n, uint32_t* pred, uint64_t* res_sum, uint64_t* cand_sum) {
     if (!c.model || !c.model->dev) fail(FGSS_ERR_INVALID, "no cost model loaded");
-    k_mlp_predict<<<grid_for(n, 256, c.num_sms * 8), 256, 0, c.stream>>>(feat, n, c.model->dev, pred,
-                                                                        (unsigned long long*)res_sum);
+    k_mlp_predict<<<grid_for(n, 256, c.num_sms * 8), 256, 0, c.stream>>>(
+        feat, n, c.model->dev, pred, (unsigned long long*)res_sum, (unsigned long long*)cand_sum);
     FGSS_LAUNCH_CK();
 }
 

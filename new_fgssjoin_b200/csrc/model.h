@@ -32,8 +32,10 @@ struct fgss_model {
 
 namespace fgss {
 
-// pred[q] <- predicted candidates (u32); *res_sum += sum of predicted results (x calib)
-void model_predict(Ctx& c, const float* feat, uint64_t n, uint32_t* pred, uint64_t* res_sum);
+// pred[q] <- predicted candidates (u32); *res_sum += sum of predicted results (x calib);
+// *cand_sum += sum of pred (when given)
+void model_predict(Ctx& c, const float* feat, uint64_t n, uint32_t* pred, uint64_t* res_sum,
+                   uint64_t* cand_sum = nullptr);
 // *out += sum of cost[0..n)
 void model_sum_cost(Ctx& c, const uint32_t* cost, uint64_t n, uint64_t* out);
 // Full-batch Adam training on (feat, target) rows already on the device;

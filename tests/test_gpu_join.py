@@ -284,3 +284,27 @@ def test_graph_replay_with_results_beyond_capture_capacity(ctx):
     got = ctx.selfjoin_batch([v], [0.9])[0]
     _check_same(got, ref2, st2)
     assert len(got) == n * (n - 1) // 2
+    # the fallback recorded the batch again in the same buffers: later calls replay it
+    for _ in range(2):
+        got = ctx.selfjoin_batch([v], [0.9])[0]
+        _check_same(got, ref2, st2)
+        assert got.stats["overflow_retries"] == 0
+
+
+def test_graph_captured_after_first_call_overflowed(ctx):
+    """A first call whose presized result buffers overflow re-runs the join
+    exactly and still captures the batch, with the exact capacity: the replays
+    give the same pairs without a re-run."""
+    a = ctx.tokenize(_titles(3000, 73), **datagen.TITLE_TOK)
+    v, arrs = _device_view(a)
+    ts = [0.5, 0.7, 0.9]
+    refs = [O.join(a.pos, a.len, a.tokens, a.n_terms, t) for t in ts]
+    first = ctx.selfjoin_batch([v] * 3, ts, result_capacity=1)
+    for got, (ref, st) in zip(first, refs):
+        _check_same(got, ref, st)
+    assert sum(o.stats["overflow_retries"] for o in first) >= 1
+    for _ in range(2):
+        outs = ctx.selfjoin_batch([v] * 3, ts, result_capacity=1)
+        for got, (ref, st) in zip(outs, refs):
+            _check_same(got, ref, st)
+            assert got.stats["overflow_retries"] == 0
