@@ -46,6 +46,8 @@ __device__ unsigned long long g_phase_cycles[8];
 // source position of the last match (11; 2047 = too large to keep) |
 // number of prefix matches (10).
 constexpr uint32_t kSmaxUnknown = 2047;
+// The warp merges together when at most this many of its lanes still merge.
+constexpr uint32_t kCoopMerges = 4;
 
 // Layout: slots u64[H] | occ u16[H] | wlo,whi,clo u32[PC] | wpre u32[PC+4] | qtok u32[QC] | bm u32[BW]
 template <int HLOG>
@@ -65,6 +67,7 @@ struct FusedLayout {
     static constexpr size_t off_qtok = off_wpre + 4ull * (PC + 4);
     static constexpr size_t off_bm = off_qtok + 4ull * QC;
     static constexpr size_t bytes = off_bm + 4ull * BW;
+    static_assert(off_bm % 16 == 0, "the membership words are cleared with 16-byte stores");
 };
 
 // Window of every probe token: warp per query.  win[poff[q] + j] = (lo, hi);
@@ -156,19 +159,55 @@ struct FusedArgs {
     const uint32_t* cbuf;    // chunk boundaries: per inner boundary, first entry of each probe window
 };
 
-__device__ __forceinline__ bool bm_test(const uint32_t* bm, bool exact, uint32_t x, const uint32_t* qtok, uint32_t qa,
-                                        uint32_t lq) {
-    const uint32_t b = exact ? x : ((x * 0x9E3779B1u) >> 17);
+// Query-token membership, three forms chosen per query (the same for every
+// thread of the CTA):
+//   QM_EXACT  vocabulary of at most 32768 terms: one bit per term;
+//   QM_HASH   larger vocabulary, query of at most 512 tokens: open-addressing
+//             set of token + 1 in the same 1024 words (load <= 1/2, 0 = empty);
+//   QM_BLOOM  otherwise: one bit per hash, hits confirmed by binary search.
+enum : uint32_t { QM_EXACT = 0, QM_HASH = 1, QM_BLOOM = 2 };
+constexpr uint32_t kQHashWords = 1024, kQHashMax = 512;
+
+__device__ __forceinline__ uint32_t qhash(uint32_t x) { return (x * 0x9E3779B1u) >> 22; }  // 10 bits
+
+__device__ __forceinline__ bool bm_test(const uint32_t* bm, uint32_t mode, uint32_t x, const uint32_t* qtok,
+                                        uint32_t qa, uint32_t lq) {
+    if (mode == QM_HASH) {
+        uint32_t h = qhash(x);
+        for (uint32_t it = 0; it < kQHashWords; it++) {
+            const uint32_t v = bm[h];
+            if (v == x + 1u) return true;
+            if (v == 0u) return false;
+            h = (h + 1u) & (kQHashWords - 1u);
+        }
+        return false;
+    }
+    const uint32_t b = mode == QM_EXACT ? x : ((x * 0x9E3779B1u) >> 17);
     bool hit = (bm[b >> 5] >> (b & 31)) & 1u;
-    if (hit && !exact) hit = contains_gen(qtok, qa, lq, x);
+    if (hit && mode != QM_EXACT) hit = contains_gen(qtok, qa, lq, x);
     return hit;
+}
+
+// Puts query token x into the membership structure of the chosen form.
+__device__ __forceinline__ void bm_insert(uint32_t* bm, uint32_t mode, uint32_t x) {
+    if (mode == QM_HASH) {
+        uint32_t h = qhash(x);
+        for (uint32_t it = 0; it < kQHashWords; it++) {
+            const uint32_t prev = atomicCAS(&bm[h], 0u, x + 1u);
+            if (prev == 0u || prev == x + 1u) return;
+            h = (h + 1u) & (kQHashWords - 1u);
+        }
+        return;
+    }
+    const uint32_t b = mode == QM_EXACT ? x : ((x * 0x9E3779B1u) >> 17);
+    atomicOr(&bm[b >> 5], 1u << (b & 31));
 }
 
 // One merge step: up to 8 source tokens from position k (two independent
 // 16-byte loads of the aligned chunks holding them; the second only when it
 // holds tokens of this record, so no load leaves the record's 16-byte blocks).
 __device__ __forceinline__ uint32_t merge_step(const uint32_t* __restrict__ st, uint32_t& k, uint32_t ls,
-                                               uint32_t xq, const uint32_t* bm, bool exact, const uint32_t* qt,
+                                               uint32_t xq, const uint32_t* bm, uint32_t mode, const uint32_t* qt,
                                                uint32_t lq) {
     const uintptr_t addr = reinterpret_cast<uintptr_t>(st + k);
     const uint4* p = reinterpret_cast<const uint4*>(addr & ~uintptr_t(15));
@@ -185,7 +224,7 @@ __device__ __forceinline__ uint32_t merge_step(const uint32_t* __restrict__ st, 
     for (uint32_t t = 0; t < 8; t++) {
         if (t >= off && t < off + n_in) {
             const uint32_t x = xs[t];
-            if (x > xq && bm_test(bm, exact, x, qt, 0, lq)) hits++;
+            if (x > xq && bm_test(bm, mode, x, qt, 0, lq)) hits++;
         }
     }
     k += n_in;
@@ -224,7 +263,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
         if (tid == 0) defer_heavy(a, q);
         return;
     }
-    const bool exact_bm = a.n_terms <= Lay::BW * 32;
+    const uint32_t qmode = a.n_terms <= Lay::BW * 32 ? QM_EXACT : (lq <= kQHashMax ? QM_HASH : QM_BLOOM);
     FGSS_PHASE_START();
     const uint32_t* qt = a.tok + qm.x;
     const bool staged = lq <= Lay::QC;
@@ -236,8 +275,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     for (uint32_t j = tid; j < lq; j += NT) {
         const uint32_t x = __ldg(qt + j);
         if (staged) qtok[j] = x;
-        const uint32_t b = exact_bm ? x : ((x * 0x9E3779B1u) >> 17);
-        atomicOr(&bm[b >> 5], 1u << (b & 31));
+        bm_insert(bm, qmode, x);
     }
     for (uint32_t j = tid; j < qp; j += NT) {
         const uint2 w = qwin[j];
@@ -450,8 +488,43 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                         }
                     }
                 }
+                // Nothing left to fetch and at most kCoopMerges merges under way: the
+                // warp takes them one after another, 32 source tokens per step
+                // (one coalesced load, a membership test per lane, ballot +
+                // popcount), with the same early exit as the lane loop.
+                if (__ballot_sync(kFull, !have && !drained) == 0) {
+                    uint32_t act = __ballot_sync(kFull, have);
+                    if (act && __popc(act) <= kCoopMerges) {
+                        while (act) {
+                            const uint32_t l = __ffs(act) - 1;
+                            act &= act - 1;
+                            const uint32_t* wst = reinterpret_cast<const uint32_t*>(
+                                __shfl_sync(kFull, reinterpret_cast<unsigned long long>(st), l));
+                            const uint32_t wls = __shfl_sync(kFull, ls, l), wxq = __shfl_sync(kFull, xq, l);
+                            const uint32_t wc = __shfl_sync(kFull, c, l), wqr = __shfl_sync(kFull, qrest, l);
+                            const uint32_t wim = __shfl_sync(kFull, im, l);
+                            uint32_t wk = __shfl_sync(kFull, k, l), wcnt = __shfl_sync(kFull, cnt, l);
+                            while (wk < wls && wcnt + min(wls - wk, wqr - (wcnt - wc)) >= wim) {
+                                const uint32_t kk = wk + lane;
+                                bool hit = false;
+                                if (kk < wls) {
+                                    const uint32_t x = __ldg(wst + kk);
+                                    hit = x > wxq && bm_test(bm, qmode, x, qsrc, 0, lq);
+                                }
+                                wcnt += __popc(__ballot_sync(kFull, hit));
+                                wk = min(wk + 32u, wls);
+                            }
+                            if (lane == l) {
+                                cnt = wcnt;
+                                k = wk;
+                                have = false;
+                                tally(cnt, k);
+                            }
+                        }
+                    }
+                }
                 if (have) {
-                    cnt += merge_step(st, k, ls, xq, bm, exact_bm, qsrc, lq);
+                    cnt += merge_step(st, k, ls, xq, bm, qmode, qsrc, lq);
                     if (k >= ls || cnt + min(ls - k, qrest - (cnt - c)) < im) {
                         have = false;
                         tally(cnt, k);
@@ -471,10 +544,15 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
         ctr.cand += s_cand;
         ctr.window += s_win;
     }
-    for (uint32_t j = tid; j < lq; j += NT) {
-        const uint32_t x = qsrc[j];
-        const uint32_t b = exact_bm ? x : ((x * 0x9E3779B1u) >> 17);
-        bm[b >> 5] = 0u;
+    if (qmode == QM_HASH) {
+        uint4* b4 = reinterpret_cast<uint4*>(bm);
+        for (uint32_t i = tid; i < kQHashWords / 4; i += NT) b4[i] = make_uint4(0, 0, 0, 0);
+    } else {
+        for (uint32_t j = tid; j < lq; j += NT) {
+            const uint32_t x = qsrc[j];
+            const uint32_t b = qmode == QM_EXACT ? x : ((x * 0x9E3779B1u) >> 17);
+            bm[b >> 5] = 0u;
+        }
     }
     __syncthreads();
 }
