@@ -293,10 +293,12 @@ def main():
     texts, jobs = workload_jobs(w, seed_offset=rank * 1000)
     train_texts = []
     if not args.no_model:
-        # a 30k-record sample of a single-file workload; 8 joins of another batch draw
-        train_texts, _ = workload_jobs(w, seed_offset=7919 + rank, n=None if w["kind"] == "batch" else 30000,
-                                       only=range(8))
-        train_texts = [x for x in train_texts if x is not None]
+        if w["kind"] == "batch":  # 8 joins of another batch draw
+            train_texts, _ = workload_jobs(w, seed_offset=7919 + rank, only=range(8))
+            train_texts = [x for x in train_texts if x is not None]
+        else:  # other samples of the workload at 1/27, 1/9 and 1/3 of its size
+            train_texts = [make_text(w, seed_offset=7919 + rank + k, n=max(1000, w["n"] // d))
+                           for k, d in enumerate((27, 9, 3))]
 
     import torch
     import new_fgssjoin_b200 as F
@@ -339,10 +341,12 @@ def main():
     model_loss = None
     if use_model:
         tr = [ctx.tokenize(x, **to) for x in train_texts]
-        k_n = max(len(tr), len(t_list))
-        model_loss = ctx.model_train([tr[k % len(tr)] for k in range(k_n)],
-                                     [t_list[k % len(t_list)] for k in range(k_n)], epochs=300, lr=0.01, seed=1)
-        del tr
+        if w["kind"] == "batch":
+            pairs = [(tr[k], t_list[k % len(t_list)]) for k in range(len(tr))]
+        else:
+            pairs = [(x, t) for x in tr for t in t_list]
+        model_loss = ctx.model_train([x for x, _ in pairs], [t for _, t in pairs], epochs=300, lr=0.01, seed=1)
+        del tr, pairs
 
     # autotuner (untimed): fastest fused-kernel shape per threshold on its largest join, cached in the context
     tuned = {}

@@ -238,7 +238,10 @@ fgss_status fgss_model_train(fgss_ctx* ctx, const fgss_sets_view* sets, const fl
                              int n, int epochs, float lr, uint64_t seed, float* final_loss);
 fgss_status fgss_model_save(fgss_ctx* ctx, const char* path);
 /* One forward + backward pass of the MLP on host arrays (n x 8 features,
- * n x 2 targets), for gradient checks: params (354 floats) -> grads, loss. */
+ * n x 2 targets = per-query counts of candidates and results), for gradient
+ * checks: params (354 floats) -> grads, loss.  The loss is the mean over rows
+ * of sum_j exp(r_j) - y_j r_j with log-rates r_j = 8 * output_j clamped to
+ * [-30, 30] (Poisson regression). */
 fgss_status fgss_model_grad(fgss_ctx* ctx, const float* feat, const float* target, uint64_t n, const float* params,
                             float* grads, float* loss);
 /* Number of MLP parameters (W1, b1, W2, b2). */

@@ -1,7 +1,10 @@
 // model.cu -- forward, backward and Adam kernels of the cost-model MLP.
 // Inputs are the per-query features of k_features (batch.cu) scaled by 1/8;
-// outputs are the two log1p targets scaled by 1/8.  Plain FP32 SIMT: the
-// network is 354 parameters, far too small for tensor cores to matter.
+// the two outputs times 8 are log-rates r of the per-query counts (candidates
+// to verify, result pairs), trained with the Poisson loss exp(r) - y r, whose
+// optimum matches the summed counts of the training joins (the output bias's
+// gradient is sum(exp(r) - y)).  Plain FP32 SIMT: the network is 354
+// parameters, far too small for tensor cores to matter.
 #include <math.h>
 #include <string.h>
 
@@ -16,6 +19,7 @@ namespace {
 
 constexpr float kInScale = 0.125f;
 constexpr float kOutScale = 8.0f;
+constexpr float kRateClamp = 30.0f;  // log-rates are clamped to [-30, 30] (zero gradient outside)
 
 __device__ __forceinline__ void mlp_fwd(const float* P, const float* x, float* hpre, float* o) {
     const float* W1 = P;
@@ -63,10 +67,12 @@ __global__ void __launch_bounds__(256) k_mlp_grad(const float* __restrict__ feat
         float l = 0.f;
 #pragma unroll
         for (int j = 0; j < kOut; j++) {
-            float y = valid ? target[i * kOut + j] / kOutScale : 0.f;
-            float d = valid ? (o[j] - y) : 0.f;
-            l += d * d;
-            dO[j] = 2.f * d * inv_n;
+            const float y = valid ? target[i * kOut + j] : 0.f;
+            const float r = o[j] * kOutScale;
+            const float rc = fminf(fmaxf(r, -kRateClamp), kRateClamp);
+            const float e = expf(rc);
+            l += valid ? e - y * rc : 0.f;
+            dO[j] = (valid && r > -kRateClamp && r < kRateClamp) ? (e - y) * kOutScale * inv_n : 0.f;
         }
         float ls = warp_sum(l);
         if (lane == 0) atomicAdd(&acc[kParams], ls * inv_n);
@@ -137,20 +143,22 @@ __global__ void __launch_bounds__(256) k_mlp_predict(const float* __restrict__ f
     for (int i = threadIdx.x; i < kParamsAll; i += blockDim.x) P[i] = Pg[i];
     __syncthreads();
     const float calib = P[kParams + 1] > 0.f ? P[kParams + 1] : 1.f;
-    unsigned long long rs = 0, cs = 0;
+    unsigned long long cs = 0;
+    double rs = 0.0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         float x[kFeatM], hpre[kHidden], o[kOut];
 #pragma unroll
         for (int f = 0; f < kFeatM; f++) x[f] = feat[i * kFeatM + f] * kInScale;
         mlp_fwd(P, x, hpre, o);
-        float lc = fminf(fmaxf(o[0] * kOutScale, 0.f), 30.f);
-        float lr = fminf(fmaxf(o[1] * kOutScale, 0.f), 30.f);
-        pred[i] = (uint32_t)fminf(expm1f(lc), 1.0e9f);
+        const float ec = expf(fminf(fmaxf(o[0] * kOutScale, -kRateClamp), kRateClamp));
+        const float er = expf(fminf(fmaxf(o[1] * kOutScale, -kRateClamp), kRateClamp));
+        pred[i] = (uint32_t)fminf(ec + 0.5f, 1.0e9f);
         cs += pred[i];
-        rs += (unsigned long long)ceilf(expm1f(lr) * calib);
+        rs += (double)er;
     }
+    // expected results: summed per warp, then rounded up once
     rs = warp_sum(rs);
-    if (lane_id() == 0 && rs) atomicAdd(res_sum, rs);
+    if (lane_id() == 0 && rs > 0.0) atomicAdd(res_sum, (unsigned long long)ceil(rs * (double)calib));
     if (cand_sum) {
         cs = warp_sum(cs);
         if (lane_id() == 0 && cs) atomicAdd(cand_sum, cs);
@@ -202,7 +210,20 @@ float model_fit(Ctx& c, const float* feat, const float* target, uint64_t n, int 
     const float s1 = sqrtf(2.f / kFeatM), s2 = sqrtf(1.f / kHidden);
     for (int i = 0; i < kHidden * kFeatM; i++) M.host[i] = nd(rng) * s1;
     float* W2 = M.host.data() + kHidden * kFeatM + kHidden;
-    for (int i = 0; i < kOut * kHidden; i++) W2[i] = nd(rng) * s2;
+    for (int i = 0; i < kOut * kHidden; i++) W2[i] = nd(rng) * s2 * 0.1f;
+    {
+        // output biases start at the log of the mean count of each head
+        std::vector<float> ht((size_t)n * kOut);
+        FGSS_CK(cudaMemcpyAsync(ht.data(), target, ht.size() * 4, cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+        float* b2 = W2 + kOut * kHidden;
+        for (int j = 0; j < kOut; j++) {
+            double m = 0.0;
+            for (uint64_t i = 0; i < n; i++) m += ht[i * kOut + j];
+            m = n ? m / (double)n : 0.0;
+            b2[j] = (float)(log(std::max(m, 1e-3)) / kOutScale);
+        }
+    }
     M.host[kParams] = 1.f;
     M.host[kParams + 1] = 1.f;
     M.dev = c.devT<float>("m.P", kParamsAll);

@@ -1,6 +1,7 @@
 // model.h -- the learned cost model of the batched method: a 2-layer FP32 MLP
 // (kFeat inputs -> kHidden ReLU -> 2 outputs) predicting, per query record,
-// log1p(candidates it must verify) and log1p(result pairs it emits).
+// the log of the expected number of candidates it must verify and of result
+// pairs it emits (Poisson regression on the exact counts).
 // Training and inference are our own CUDA kernels (model.cu).  The model is
 // advisory only: it sizes the result buffers and balances work items; an
 // undersized buffer is detected on the device and the join re-runs exactly.

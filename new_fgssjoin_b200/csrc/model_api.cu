@@ -28,13 +28,13 @@ __global__ void k_res_hist(const uint32_t* __restrict__ oq, uint64_t R, uint32_t
 __global__ void k_targets(const uint32_t* __restrict__ vcnt, const uint32_t* __restrict__ rcnt, uint64_t n,
                           float* __restrict__ target) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        target[2 * i] = log1pf((float)vcnt[i]);
-        target[2 * i + 1] = log1pf((float)rcnt[i]);
+        target[2 * i] = (float)vcnt[i];
+        target[2 * i + 1] = (float)rcnt[i];
     }
 }
 
 const uint32_t kMagic = 0x4d535346u;  // "FSSM"
-const uint32_t kFormat = 1;
+const uint32_t kFormat = 2;  // 2: Poisson log-rate outputs (1 held log1p outputs)
 
 }  // namespace
 

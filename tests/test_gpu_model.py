@@ -24,17 +24,20 @@ def _unpack(p):
 
 
 def _np_loss_grad(feat, target, p):
-    """Float64 reference: mean over rows of the summed squared error of the scaled outputs."""
+    """Float64 reference: mean over rows of the Poisson loss sum_j exp(r_j) - y_j r_j,
+    with log-rates r = 8 * output clamped to [-30, 30] (zero gradient outside)."""
     W1, b1, W2, b2 = _unpack(p)
     x = feat.astype(np.float64) * IN_SCALE
-    y = target.astype(np.float64) / OUT_SCALE
+    y = target.astype(np.float64)
     hp = x @ W1.T + b1
     h = np.maximum(hp, 0)
     o = h @ W2.T + b2
     n = x.shape[0]
-    d = o - y
-    loss = (d ** 2).sum() / n
-    dO = 2 * d / n
+    r = o * OUT_SCALE
+    rc = np.clip(r, -30.0, 30.0)
+    e = np.exp(rc)
+    loss = (e - y * rc).sum() / n
+    dO = np.where((r > -30.0) & (r < 30.0), (e - y) * OUT_SCALE, 0.0) / n
     gW2 = dO.T @ h
     gb2 = dO.sum(0)
     dh = (dO @ W2) * (hp > 0)
@@ -51,8 +54,8 @@ def test_num_params():
 def test_gradients_match_float64_oracle(ctx, n):
     rng = np.random.default_rng(n)
     feat = rng.uniform(0, 12, (n, NF)).astype(np.float32)
-    target = rng.uniform(0, 10, (n, NO)).astype(np.float32)
-    params = (rng.standard_normal(NH * NF + NH + NO * NH + NO) * 0.3).astype(np.float32)
+    target = np.floor(rng.exponential(20.0, (n, NO))).astype(np.float32)  # counts
+    params = (rng.standard_normal(NH * NF + NH + NO * NH + NO) * 0.1).astype(np.float32)
     g, loss = ctx.model_grad(feat, target, params)
     rl, rg = _np_loss_grad(feat, target, params)
     assert abs(loss - rl) <= 1e-4 * max(1.0, abs(rl))
@@ -102,3 +105,34 @@ def test_undersized_result_buffer_reruns_exactly(ctx, titles):
     assert got.stats["overflow_retries"] == 1
     assert np.array_equal(got.q, ref["q"]) and np.array_equal(got.s, ref["s"])
     assert got.stats["candidates"] == st["candidates"]
+
+
+def _dup_titles(n_distinct, copies, seed):
+    """Title records, each line repeated `copies` times in a row."""
+    lines = datagen.titles(n_distinct, seed=seed).split(b"\n")[:-1]
+    return b"\n".join(x for x in lines for _ in range(copies)) + b"\n"
+
+
+def test_trained_model_gains_one_filter_pass(ctx):
+    """What the trained network gains over the method without it: on records with
+    many duplicates the result pairs outnumber the records, so the model-free
+    result buffer (records + 4096 slots) overflows and the join runs its filter
+    a second time with the exact size; with the trained model the presized
+    buffer fits and the filter runs once.  The pair set is the same."""
+    train = ctx.tokenize(_dup_titles(3000, 6, 51), **datagen.TITLE_TOK)
+    test = ctx.tokenize(_dup_titles(3000, 6, 52), **datagen.TITLE_TOK)
+    ref, st = O.join(test.pos, test.len, test.tokens, test.n_terms, 0.8)
+    assert st["results"] > test.n_sets + 4096
+    outs = {}
+    for learned in (False, True):
+        with F.Context(device=0) as fresh:  # nothing remembered from earlier calls
+            if learned:
+                fresh.model_train([train], [0.8], epochs=300, lr=0.01, seed=1)
+            outs[learned] = fresh.selfjoin(test, 0.8, method="batched", use_model=learned)
+    assert outs[False].stats["overflow_retries"] == 1
+    assert outs[True].stats["overflow_retries"] == 0
+    pred = outs[True].stats["predicted_results"]
+    assert 0.5 * st["results"] <= pred <= 2.0 * st["results"], (pred, st["results"])
+    for got in outs.values():
+        assert np.array_equal(got.q, ref["q"]) and np.array_equal(got.s, ref["s"])
+        assert got.stats["candidates"] == st["candidates"]
