@@ -192,6 +192,45 @@ def test_long_records_take_the_heavy_path(ctx):
         assert got.stats["heavy_queries"] > 0
 
 
+def _sets_of(recs, n_terms):
+    recs = sorted(recs, key=len, reverse=True)  # memory order: descending size
+    lens = np.array([len(r) for r in recs])
+    pos = np.concatenate([[0], np.cumsum(lens[:-1])])
+    return F.Sets(np.arange(1, len(recs) + 1), pos, lens, np.concatenate(recs).astype(np.uint32), n_terms)
+
+
+def test_large_vocabulary_long_records_vs_oracle(ctx):
+    """Vocabulary above 32,768 terms: queries of up to 512 tokens use the hashed
+    query set, longer ones the hashed bitmap confirmed by binary search; near
+    copies make long merges (the warp-cooperative path)."""
+    rng = np.random.default_rng(21)
+    V = 200000
+    recs = []
+    for _ in range(40):
+        b = np.sort(rng.choice(V, int(rng.integers(300, 1100)), replace=False))
+        recs.append(b)
+        for _ in range(3):
+            keep = b[rng.random(len(b)) > 0.04]
+            recs.append(np.unique(np.concatenate([keep, rng.choice(V, 8, replace=False)])))
+    for _ in range(300):
+        recs.append(np.sort(rng.choice(V, int(rng.integers(5, 80)), replace=False)))
+    s = _sets_of(recs, V)
+    for t in (0.7, 0.9):
+        ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, t)
+        assert st["results"] > 50
+        for method in ("plain", "batched"):
+            _check_same(ctx.selfjoin(s, t, method=method), ref, st)
+
+
+@pytest.mark.parametrize("t", [0.6, 0.8])
+def test_heavy_tailed_records_vs_oracle(ctx, t):
+    """The heavy-tailed generator (lognormal sizes, near-duplicate clusters) at a small size."""
+    s = ctx.tokenize(datagen.heavy(4000, seed=9), **datagen.TITLE_TOK)
+    ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, t)
+    for method in ("plain", "batched"):
+        _check_same(ctx.selfjoin(s, t, method=method), ref, st)
+
+
 def test_kmer_reads_vs_oracle(ctx):
     text = datagen.reads(3000, seed=3, genome_len=60000)
     s = ctx.tokenize(text, **datagen.READ_TOK)
