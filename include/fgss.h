@@ -132,6 +132,15 @@ void fgss_tok_opts_default(fgss_tok_opts* o);
 fgss_status fgss_tokenize(fgss_ctx* ctx, const char* text, uint64_t n_bytes,
                           const fgss_tok_opts* opts, fgss_sets* out);
 
+/* Two texts tokenized over one vocabulary (the text of R, then the text of S,
+ * as one input to fgss_tokenize): term ids by document frequency over both.
+ * out_r and out_s get the records of each text in MEMORY order, ids counting
+ * the non-empty lines of their own text, n_terms of the shared vocabulary.
+ * The reference's preprocess CLI has a "dualjoin" mode with this purpose
+ * (src/preprocess_cli.cpp:22-32,93-119) that reads only its first file. */
+fgss_status fgss_tokenize_dual(fgss_ctx* ctx, const char* text_r, uint64_t n_r, const char* text_s,
+                               uint64_t n_s, const fgss_tok_opts* opts, fgss_sets* out_r, fgss_sets* out_s);
+
 /* ------------------------------------------------------------------ join */
 
 enum { FGSS_BOUNDS_REFERENCE = 0, /* float32 bounds exactly as similarity.cuh:9-82 */
@@ -228,6 +237,20 @@ typedef struct fgss_tune_result {
  * batched joins of the same class use it.  No reference counterpart. */
 fgss_status fgss_autotune(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_join_opts* opts, int reps,
                           fgss_tune_result* best);
+
+/* R-S join: every pair (r, s), r a record of R and s a record of S over one
+ * vocabulary (fgss_tokenize_dual), with Jaccard >= t.  No reference
+ * counterpart (the reference's "dualjoin" stops at tokenizing).  Defined as
+ * the self-join of R and S together -- the union in memory order: descending
+ * size, R before S at equal size, then the index within its side -- restricted
+ * to pairs with one record from each side; so FGSS_BOUNDS_EXACT gives exactly
+ * the pairs with J >= t, and the reference bounds the self-join's float32
+ * boundary behaviour.  Pairs are (q = index in R, s = index in S), sorted by
+ * (q, s); the counters count pairs across only.  opts: threshold, bounds,
+ * method (plain or batched), use_model, result_capacity, out_on_device;
+ * query ranges and want_candidates are rejected. */
+fgss_status fgss_rsjoin(fgss_ctx* ctx, const fgss_sets_view* r, const fgss_sets_view* s,
+                        const fgss_join_opts* opts, fgss_pairs* out, fgss_stats* stats);
 
 /* ------------------------------------------------------- learned cost model */
 

@@ -15,8 +15,9 @@ TOK_QGRAM, TOK_KMER = 0, 1
 EXPORTED_SYMBOLS = [
     "fgss_options_default", "fgss_create", "fgss_destroy", "fgss_strerror", "fgss_last_error", "fgss_version",
     "fgss_load_bin", "fgss_write_bin", "fgss_sets_free", "fgss_sets_view_of",
-    "fgss_tok_opts_default", "fgss_tokenize",
-    "fgss_join_opts_default", "fgss_selfjoin", "fgss_selfjoin_batch", "fgss_pairs_free", "fgss_pairs_print",
+    "fgss_tok_opts_default", "fgss_tokenize", "fgss_tokenize_dual",
+    "fgss_join_opts_default", "fgss_selfjoin", "fgss_selfjoin_batch", "fgss_rsjoin", "fgss_pairs_free",
+    "fgss_pairs_print",
     "fgss_model_train", "fgss_model_save", "fgss_model_load", "fgss_model_grad", "fgss_model_num_params",
     "fgss_autotune", "fgss_bounds_table", "fgss_dev_exclusive_scan_u32", "fgss_dev_sort_pairs_u64",
     "fgss_dev_exclusive_scan_u32_noalloc",
@@ -111,6 +112,9 @@ def load_library():
     L.fgss_tokenize.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64, P(_TokOpts), P(_Sets)]
     L.fgss_selfjoin.argtypes = [ctypes.c_void_p, P(_View), P(_JoinOpts), P(_Pairs), P(_Stats)]
     L.fgss_selfjoin_batch.argtypes = [ctypes.c_void_p, P(_View), P(_JoinOpts), ctypes.c_int, P(_Pairs), P(_Stats)]
+    L.fgss_tokenize_dual.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_char_p,
+                                     ctypes.c_uint64, P(_TokOpts), P(_Sets), P(_Sets)]
+    L.fgss_rsjoin.argtypes = [ctypes.c_void_p, P(_View), P(_View), P(_JoinOpts), P(_Pairs), P(_Stats)]
     L.fgss_pairs_free.argtypes = [P(_Pairs)]
     L.fgss_model_train.argtypes = [ctypes.c_void_p, P(_View), P(ctypes.c_float), ctypes.c_int, ctypes.c_int,
                                    ctypes.c_float, ctypes.c_uint64, P(ctypes.c_float)]
@@ -307,6 +311,21 @@ class Context:
         finally:
             self._L.fgss_sets_free(ctypes.byref(s))
 
+    def tokenize_dual(self, text_r, text_s, q=3, mode="qgram", pad=False, pad_char=1, suffix=True, lower=True):
+        """Two texts over one vocabulary -> (Sets of R, Sets of S) (fgss_tokenize_dual)."""
+        text_r = text_r.encode("latin-1") if isinstance(text_r, str) else text_r
+        text_s = text_s.encode("latin-1") if isinstance(text_s, str) else text_s
+        o = _TokOpts(q, TOK_KMER if mode == "kmer" else TOK_QGRAM, int(pad), pad_char, int(suffix), int(lower))
+        a, b = _Sets(), _Sets()
+        st = self._L.fgss_tokenize_dual(self._ctx, text_r, len(text_r), text_s, len(text_s), ctypes.byref(o),
+                                        ctypes.byref(a), ctypes.byref(b))
+        _check(self._L, self._ctx, st)
+        try:
+            return Sets._from_c(a), Sets._from_c(b)
+        finally:
+            self._L.fgss_sets_free(ctypes.byref(a))
+            self._L.fgss_sets_free(ctypes.byref(b))
+
     # ----------------------------------------------------------------- join
     @staticmethod
     def _opts(threshold, method, bounds, want_candidates, use_model, out_on_device=False, result_capacity=0,
@@ -353,6 +372,19 @@ class Context:
         rc = self._L.fgss_selfjoin(self._ctx, ctypes.byref(v), ctypes.byref(o), ctypes.byref(p), ctypes.byref(st))
         _check(self._L, self._ctx, rc)
         return self._collect(p, st, want_candidates)
+
+    def rsjoin(self, r, s, threshold, method="batched", bounds="reference", use_model=False, result_capacity=0):
+        """R-S join (fgss_rsjoin): pairs (index in R, index in S) with Jaccard >= threshold,
+        returned with ``q`` = the R index and ``s`` = the S index, sorted by (q, s)."""
+        vr = r.view() if isinstance(r, Sets) else r
+        vs = s.view() if isinstance(s, Sets) else s
+        o = self._opts(threshold, method, bounds, False, use_model, result_capacity=result_capacity)
+        p = _Pairs()
+        st = _Stats()
+        rc = self._L.fgss_rsjoin(self._ctx, ctypes.byref(vr), ctypes.byref(vs), ctypes.byref(o), ctypes.byref(p),
+                                 ctypes.byref(st))
+        _check(self._L, self._ctx, rc)
+        return self._collect(p, st, False)
 
     def selfjoin_batch(self, sets_list, thresholds, method="batched", bounds="reference", use_model=False,
                        result_capacity=0):

@@ -526,6 +526,106 @@ fgss_status fgss_tokenize(fgss_ctx* ctx, const char* text, uint64_t n_bytes, con
     });
 }
 
+fgss_status fgss_tokenize_dual(fgss_ctx* ctx, const char* text_r, uint64_t n_r, const char* text_s, uint64_t n_s,
+                               const fgss_tok_opts* opts, fgss_sets* out_r, fgss_sets* out_s) {
+    if (!ctx || !out_r || !out_s || (!text_r && n_r) || (!text_s && n_s)) return FGSS_ERR_INVALID;
+    memset(out_r, 0, sizeof *out_r);
+    memset(out_s, 0, sizeof *out_s);
+    return guard(ctx, [&] {
+        fgss_tok_opts o;
+        fgss_tok_opts_default(&o);
+        if (opts) o = *opts;
+        TokParams p{o.q, o.mode, o.pad, o.pad_char, o.suffix, o.lower};
+        FGSS_CK(cudaSetDevice(ctx->c.device));
+        // one text: R's lines, then S's; record ids count the non-empty lines
+        std::string text(text_r ? text_r : "", n_r);
+        uint32_t nr_lines = 0;
+        for (uint64_t i = 0; i < n_r;) {
+            uint64_t e = i;
+            while (e < n_r && text_r[e] != '\n') e++;
+            if (e > i) nr_lines++;
+            i = e + 1;
+        }
+        if (n_r && text_r[n_r - 1] != '\n') text.push_back('\n');
+        if (n_s) text.append(text_s, n_s);
+        fgss_sets all;
+        memset(&all, 0, sizeof all);
+        try {
+            tokenize_device(ctx->c, text.data(), text.size(), p, &all);
+            fgss_sets* outs[2] = {out_r, out_s};
+            uint64_t cnt[2] = {0, 0}, tok[2] = {0, 0};
+            for (uint64_t i = 0; i < all.n_sets; i++) {
+                const int sd = all.id[i] > nr_lines;
+                cnt[sd]++;
+                tok[sd] += all.len[i];
+            }
+            for (int sd = 0; sd < 2; sd++) {
+                fgss_sets& d = *outs[sd];
+                d.n_sets = cnt[sd];
+                d.n_tokens = tok[sd];
+                d.n_terms = all.n_terms;
+                const size_t nb = (cnt[sd] ? cnt[sd] : 1) * 4, tb = (tok[sd] ? tok[sd] : 1) * 4;
+                d.id = (uint32_t*)malloc(nb);
+                d.pos = (uint32_t*)malloc(nb);
+                d.len = (uint32_t*)malloc(nb);
+                d.tokens = (uint32_t*)malloc(tb);
+                d.loc = all.loc ? (uint32_t*)malloc(tb) : nullptr;
+                if (!d.id || !d.pos || !d.len || !d.tokens || (all.loc && !d.loc))
+                    fail(FGSS_ERR_NOMEM, "host allocation for token sets");
+            }
+            uint64_t at[2] = {0, 0}, ti[2] = {0, 0};
+            for (uint64_t i = 0; i < all.n_sets; i++) {
+                const int sd = all.id[i] > nr_lines;
+                fgss_sets& d = *outs[sd];
+                const uint64_t k = at[sd]++, l = all.len[i];
+                d.id[k] = sd ? all.id[i] - nr_lines : all.id[i];
+                d.pos[k] = (uint32_t)ti[sd];
+                d.len[k] = (uint32_t)l;
+                memcpy(d.tokens + ti[sd], all.tokens + all.pos[i], l * 4);
+                if (d.loc) memcpy(d.loc + ti[sd], all.loc + all.pos[i], l * 4);
+                d.max_len = std::max<uint32_t>(d.max_len, (uint32_t)l);
+                ti[sd] += l;
+            }
+        } catch (...) {
+            fgss_sets_free(&all);
+            fgss_sets_free(out_r);
+            fgss_sets_free(out_s);
+            throw;
+        }
+        fgss_sets_free(&all);
+    });
+}
+
+fgss_status fgss_rsjoin(fgss_ctx* ctx, const fgss_sets_view* r, const fgss_sets_view* s, const fgss_join_opts* opts,
+                        fgss_pairs* out, fgss_stats* stats) {
+    if (!ctx || !r || !s || !opts || !out) return FGSS_ERR_INVALID;
+    return guard(ctx, [&] {
+        Ctx& c = ctx->c;
+        FGSS_CK(cudaSetDevice(c.device));
+        if (opts->want_candidates) fail(FGSS_ERR_INVALID, "want_candidates is for self-joins");
+        if (opts->query_end > opts->query_begin) fail(FGSS_ERR_INVALID, "query ranges are for self-joins");
+        cudaEvent_t* ev = c.ev;
+        const unsigned long long launches0 = launch_counter();
+        c.probe_timed = false;
+        FGSS_CK(cudaEventRecord(ev[0], c.stream));
+        const RsInput u = rs_union(c, *r, *s);
+        JoinState J;
+        J.ns = "rs.";
+        join_setup(c, J, u.view, *opts, 0);
+        J.args.side = u.side;
+        join_index(c, J);
+        FGSS_CK(cudaEventRecord(ev[1], c.stream));
+        std::vector<JoinState*> v{&J};
+        if (opts->method == FGSS_METHOD_BATCHED) batched_filter_verify(c, v, opts->use_model != 0, nullptr);
+        else join_plain_filter_verify(c, J, false);
+        FGSS_CK(cudaEventRecord(ev[2], c.stream));
+        join_finish_status(c, J);
+        rs_output(c, J, u);
+        export_pairs(c, J, *opts, out);
+        report_stats(c, v, stats, launch_counter() - launches0, 1);
+    });
+}
+
 fgss_status fgss_selfjoin(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_join_opts* opts, fgss_pairs* out,
                           fgss_stats* stats) {
     if (!ctx || !sets || !opts || !out) return FGSS_ERR_INVALID;

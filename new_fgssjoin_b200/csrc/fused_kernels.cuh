@@ -264,6 +264,8 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
         return;
     }
     const uint32_t qmode = a.n_terms <= Lay::BW * 32 ? QM_EXACT : (lq <= kQHashMax ? QM_HASH : QM_BLOOM);
+    const uint8_t* sidep = a.side;  // R-S join: skip sources on the query's own side
+    const uint8_t side_q = sidep ? __ldg(sidep + q) : 0;
     FGSS_PHASE_START();
     const uint32_t* qt = a.tok + qm.x;
     const bool staged = lq <= Lay::QC;
@@ -388,6 +390,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                     const uint32_t s = sv[u];
                     if (s == kEmpty) continue;
                     if (unsorted && !size_ok(a, lq, a.len[s])) continue;
+                    if (sidep && __ldg(sidep + s) == side_q) continue;
                     const uint32_t pos = jv[u];  // query position << 11 | source position
                     uint32_t h = hash_slot(s, hl);
                     bool done = false;

@@ -61,6 +61,20 @@ struct JoinState {
 };
 
 // Stage drivers (join.cu)
+// R-S join input (rsjoin.cu): the union of R and S in memory order, the side
+// of every union record (0 = R, 1 = S) and its index within that side.
+struct RsInput {
+    fgss_sets_view view{};               // the union, device memory
+    uint8_t* side = nullptr;
+    uint32_t* orig = nullptr;
+    uint64_t nr = 0, ns = 0;
+    const uint32_t* rid = nullptr;       // the sides' record ids on the device (or null)
+    const uint32_t* sid = nullptr;
+};
+RsInput rs_union(Ctx& c, const fgss_sets_view& r, const fgss_sets_view& s);
+// After join_output: pairs as (index in R, index in S), sorted by that.
+void rs_output(Ctx& c, JoinState& J, const RsInput& u);
+
 // Queues the input validation and the per-record counts of one join.  With
 // check=false the caller synchronizes the stream once for a whole batch and
 // then calls join_check_input for every join before any kernel reads tokens.

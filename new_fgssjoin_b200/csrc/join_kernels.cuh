@@ -97,6 +97,9 @@ struct JoinArgs {
     uint32_t q_lo;             // queries processed: [q_lo, q_hi) (a shard of the join)
     uint32_t q_hi;
     uint32_t pad_;
+    // R-S join: one byte per record (0 = R, 1 = S); pairs within one side are
+    // skipped before any filter.  nullptr for a self-join.
+    const uint8_t* side;
 };
 
 // ------------------------------------------------------------ small helpers
@@ -585,6 +588,7 @@ __device__ void probe_query_smem(const JoinArgs& a, uint32_t q, unsigned char* s
             const uint32_t k = clo[j] + (f - wpre[j]);
             const uint32_t s = __ldg(a.ent_s + k);
             if (unsorted && !size_ok(a, lq, a.len[s])) continue;
+            if (a.side && __ldg(a.side + s) == __ldg(a.side + q)) continue;
             if (!slot_add(slots, mask, hl, s, j)) atomicOr(a.status, ST_HASH_FULL);
         }
         __syncthreads();
@@ -769,6 +773,7 @@ __global__ void __launch_bounds__(NT) k_probe_heavy(const JoinArgs* __restrict__
             uint32_t s = __ldg(a.ent_s + k);
             uint32_t sp = __ldg(a.ent_p + k);
             if (unsorted && !size_ok(a, lq, a.len[s])) continue;
+            if (a.side && __ldg(a.side + s) == __ldg(a.side + q)) continue;
             uint32_t old = atomicAdd(&gcnt[s], 1u);
             if (old == 0) gtouch[atomicAdd(&s_nt, 1u)] = s;
             atomicMax(&gmp[s], (j << 16) | sp);

@@ -325,6 +325,9 @@ static void pv_push(pairvec* v, orc_pair x)
  *               covering every record.
  *   q_lo, q_hi: only queries (first records of pairs) in [q_lo, q_hi); 0, 0 = all
  *               (a shard of the join, for the multi-GPU tests).
+ *   side:       NULL, or one byte per record; pairs of records with the same
+ *               side byte are skipped before any filter (the R-S join as the
+ *               self-join of R and S together restricted to pairs across).
  *   want_cands: if nonzero, *cands receives every candidate as
  *               (q, s, partial score) triples -- the cells with score > 0
  *               after filtering (filtering.cu:52-57 / compaction.cu:8-17).
@@ -333,7 +336,7 @@ static void pv_push(pairvec* v, orc_pair x)
 int64_t orc_join(const uint32_t* pos, const uint32_t* len, const uint32_t* tokens,
                  uint32_t n, uint32_t n_terms, float t, uint32_t block_size, int nthreads,
                  orc_pair** out, orc_stats* st, int want_cands, uint32_t** cands, uint64_t* n_cands,
-                 uint32_t q_lo, uint32_t q_hi)
+                 uint32_t q_lo, uint32_t q_hi, const uint8_t* side)
 {
     if (!(t > 0.0f && t < 1.0f)) return -ORC_ERR_ARG;
     memset(st, 0, sizeof(*st));
@@ -406,6 +409,7 @@ int64_t orc_join(const uint32_t* pos, const uint32_t* len, const uint32_t* token
                         uint32_t source = ent_s[k], source_tpos = ent_p[k];
                         g_probe++;
                         if (!(query < source && source >= i_offset && source < i_offset + block_size)) continue;
+                        if (side && side[source] == side[query]) continue;
                         uint32_t source_len = len[source];
                         uint32_t s_min = (uint32_t)floorf(jac_min_size_f(source_len, t));
                         uint32_t s_max = (uint32_t)floorf(jac_max_size_f(source_len, t));

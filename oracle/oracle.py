@@ -50,7 +50,8 @@ def lib():
         L.orc_tokenize.restype = ctypes.c_int
         L.orc_join.argtypes = [u32p, u32p, u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
                                ctypes.c_uint32, ctypes.c_int, P(P(_Pair)), P(_Stats), ctypes.c_int,
-                               P(u32p), P(ctypes.c_uint64), ctypes.c_uint32, ctypes.c_uint32]
+                               P(u32p), P(ctypes.c_uint64), ctypes.c_uint32, ctypes.c_uint32,
+                               P(ctypes.c_uint8)]
         L.orc_join.restype = ctypes.c_int64
         L.orc_brute.argtypes = [u32p, u32p, u32p, ctypes.c_uint32, ctypes.c_float, P(P(_Pair))]
         L.orc_brute.restype = ctypes.c_int64
@@ -151,7 +152,8 @@ def encode_bin(ids, lens, tokens):
     return np.concatenate(out).tobytes() if out else b""
 
 
-def join(pos, lens, tokens, n_terms, t, block_size=0, threads=0, want_candidates=False, query_range=None):
+def join(pos, lens, tokens, n_terms, t, block_size=0, threads=0, want_candidates=False, query_range=None,
+         side=None):
     """Reference-semantics self-join on MEMORY-order records.
 
     Returns (pairs, stats[, candidates]) where pairs is a structured array
@@ -169,9 +171,13 @@ def join(pos, lens, tokens, n_terms, t, block_size=0, threads=0, want_candidates
     ncand = ctypes.c_uint64()
     nthreads = threads if threads > 0 else L.orc_num_threads()
     qb, qe = query_range if query_range else (0, 0)
+    side_p = None
+    if side is not None:
+        side_a = np.ascontiguousarray(side, dtype=np.uint8)
+        side_p = side_a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
     n = L.orc_join(pp, lp, tp, len(len_a), int(n_terms), ctypes.c_float(t), block_size, nthreads,
                    ctypes.byref(out), ctypes.byref(st), int(want_candidates), ctypes.byref(cptr),
-                   ctypes.byref(ncand), int(qb), int(qe))
+                   ctypes.byref(ncand), int(qb), int(qe), side_p)
     if n < 0:
         raise ValueError("orc_join failed: %d" % n)
     pairs = _pairs(out, n)
@@ -218,3 +224,65 @@ def bounds_table(t, maxlen):
             np.array([L.orc_mid_prefix(ft, int(i)) for i in n], np.uint32),
             np.array([L.orc_min_size(ft, int(i)) for i in n], np.uint32),
             np.array([L.orc_max_size(ft, int(i)) for i in n], np.uint32))
+
+
+def rs_union(r_len, s_len):
+    """Memory order of the union of two record sets (each in memory order):
+    descending size, then R before S, then the index within its side.
+    Returns (side u8, index within side u32) per union record."""
+    r_len = np.asarray(r_len, dtype=np.int64)
+    s_len = np.asarray(s_len, dtype=np.int64)
+    ln = np.concatenate([r_len, s_len])
+    side = np.concatenate([np.zeros(len(r_len), np.uint8), np.ones(len(s_len), np.uint8)])
+    idx = np.concatenate([np.arange(len(r_len)), np.arange(len(s_len))]).astype(np.int64)
+    order = np.lexsort((idx, side, -ln))
+    return side[order], idx[order].astype(np.uint32)
+
+
+RS_PAIR_DTYPE = np.dtype([("r", "<u4"), ("s", "<u4"), ("overlap", "<u4"), ("sim", "<f4")])
+
+
+def rsjoin(r, s, n_terms, t, threads=0):
+    """R-S join as defined by the library: the self-join of R and S together (union
+    in rs_union order) restricted to pairs with one record from each side, each
+    reported as (index in R, index in S) and sorted by (r, s).  ``r`` and ``s`` are
+    (pos, len, tokens) in memory order over one vocabulary.  Returns (pairs, stats)."""
+    (rp, rl, rt), (sp, sl, stk) = r, s
+    rp, rl, rt = (np.asarray(x, dtype=np.uint32) for x in (rp, rl, rt))
+    sp, sl, stk = (np.asarray(x, dtype=np.uint32) for x in (sp, sl, stk))
+    side, idx = rs_union(rl, sl)
+    m = side == 0
+    ulen = np.empty(len(side), np.uint32)
+    upos = np.empty(len(side), np.uint32)
+    ulen[m], upos[m] = rl[idx[m]], rp[idx[m]]
+    ulen[~m], upos[~m] = sl[idx[~m]], sp[idx[~m]] + len(rt)
+    utok = np.concatenate([rt, stk]).astype(np.uint32)
+    pairs, st = join(upos, ulen, utok, n_terms, t, threads=threads, side=side)
+    out = np.zeros(len(pairs), dtype=RS_PAIR_DTYPE)
+    if len(pairs):
+        q, v = pairs["q"], pairs["s"]
+        q_is_r = side[q] == 0
+        out["r"] = np.where(q_is_r, idx[q], idx[v])
+        out["s"] = np.where(q_is_r, idx[v], idx[q])
+        out["overlap"] = pairs["overlap"]
+        out["sim"] = pairs["sim"]
+        out = out[np.lexsort((out["s"], out["r"]))]
+    return out, st
+
+
+def rs_brute(r, s, t):
+    """All R x S pairs with float(o) / float(|r| + |s| - o) >= t and o > 0 (the
+    reference's final test, block.cu:190-193), sorted by (r, s); small inputs only."""
+    (rp, rl, rt), (sp, sl, stk) = r, s
+    res = []
+    rsets = [np.asarray(rt[int(p):int(p) + int(n)]) for p, n in zip(rp, rl)]
+    ssets = [np.asarray(stk[int(p):int(p) + int(n)]) for p, n in zip(sp, sl)]
+    for i, a in enumerate(rsets):
+        for j, b in enumerate(ssets):
+            o = len(np.intersect1d(a, b, assume_unique=True))
+            if o == 0:
+                continue
+            sim = np.float32(o) / np.float32(len(a) + len(b) - o)
+            if sim >= np.float32(t):
+                res.append((i, j, o, sim))
+    return np.array(res, dtype=RS_PAIR_DTYPE)

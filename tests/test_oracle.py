@@ -80,3 +80,30 @@ def test_float32_bounds_differ_from_exact_where_expected():
     """At t = 0.8 a 135-token read gets an index prefix of 15 (16 exactly)."""
     assert O.lib().orc_mid_prefix(np.float32(0.8), 135) == 15
     assert O.lib().orc_mid_prefix(np.float32(0.7), 135) == 135 - int(np.ceil(2 * 0.7 / 1.7 * 135)) + 1
+
+
+def test_rs_union_order():
+    side, idx = O.rs_union([5, 3, 3, 1], [4, 3, 2])
+    # descending size, R before S at equal size, then index within the side
+    assert side.tolist() == [0, 1, 0, 0, 1, 1, 0]
+    assert idx.tolist() == [0, 0, 1, 2, 1, 2, 3]
+
+
+@pytest.mark.parametrize("t", [0.5, 0.7, 0.8, 0.9])
+def test_rsjoin_equals_brute_force(t):
+    """The R-S join (self-join of the union restricted to pairs across) against
+    all R x S pairs; equal wherever the float32 bounds lose no pair (t = 0.8 is
+    checked as a subset, as for the self-join)."""
+    from rs_util import split_titles, oracle_dual
+    tr, ts = split_titles(2400, 7)
+    (rid, rp, rl, rt), (sid, sp, sl, stk), nt = oracle_dual(tr, ts, q=3, pad=True, suffix=False)
+    got, st = O.rsjoin((rp, rl, rt), (sp, sl, stk), nt, t)
+    ref = O.rs_brute((rp, rl, rt), (sp, sl, stk), t)
+    assert st["results"] == len(got) and len(ref) > 0
+    key = lambda a: set(zip(a["r"].tolist(), a["s"].tolist()))
+    assert key(got) <= key(ref)
+    if t != 0.8:
+        assert key(got) == key(ref)
+    m = {(r, s): (o, x) for r, s, o, x in ref.tolist()}
+    for r, s, o, x in got.tolist():
+        assert m[(r, s)] == (o, x)
