@@ -13,6 +13,8 @@ Other workloads:
              each with its own t from {0.6, 0.7, 0.8, 0.9, 0.95}; one step = the 256
              joins, batched in one call against 256 sequential plain calls, with the
              per-join latency p50/p99 of both forms;
+  rs200k     R-S join: 200,000 title records dealt alternately into R and S (one
+             vocabulary), t in {0.6, 0.8} (no counterpart in the reference);
   titles18k, heavy300k  smaller cases (the 18k-title join at t = 0.9; a profiling size).
 
 Metric: candidates per second (candidates = the reference's "# Candidates"
@@ -21,7 +23,7 @@ per-stage form is timed on the same step and reported beside it, with a check
 that both pair sets are identical.
 
   python bench.py [--gpus N] [--steps K] [--warmup W]
-                  [--workload titles100k|heavy1m|reads500k|batch256|titles18k|heavy300k]
+                  [--workload titles100k|heavy1m|reads500k|batch256|rs200k|titles18k|heavy300k]
                   [--thresholds 0.7,0.9] [--no-model] [--no-tune] [--no-cpu-baseline]
   python bench.py --impl reference ...   # the CPU restatement of the reference algorithm
 """
@@ -42,6 +44,7 @@ WORKLOADS = {
     "heavy1m": dict(kind="heavy", n=1_000_000, seed=3, thresholds=[0.7]),
     "reads500k": dict(kind="reads", n=500_000, seed=5, thresholds=[0.8]),
     "batch256": dict(kind="batch", joins=256, lo=1000, hi=200_000, seed=6),
+    "rs200k": dict(kind="rs", n=200_000, seed=8, thresholds=[0.6, 0.8]),
     "titles18k": dict(kind="titles", n=18_000, seed=1, thresholds=[0.9]),
     "heavy300k": dict(kind="heavy", n=300_000, seed=4, thresholds=[0.7]),  # profiling size: > L2, a few GB
 }
@@ -53,7 +56,7 @@ def make_text(w, seed_offset=0, n=None):
     smaller read sample keeps the genome's coverage by shrinking the genome)."""
     from new_fgssjoin_b200 import datagen
     n = n or w["n"]
-    if w["kind"] == "titles":
+    if w["kind"] in ("titles", "rs"):
         return datagen.titles(n, seed=w["seed"] + seed_offset)
     if w["kind"] == "reads":
         return datagen.reads(n, seed=w["seed"] + seed_offset, genome_len=max(10_000, GENOME_LEN * n // w["n"]))
@@ -72,6 +75,9 @@ def workload_jobs(w, seed_offset=0, n=None, only=None):
     threshold per join (datagen.batch_sizes); its files are generated in a
     spawned process pool before the first GPU call.  ``only``: the file
     indices to generate (the others are None)."""
+    if w["kind"] == "rs":  # one title file dealt alternately into R and S
+        lines = make_text(w, seed_offset, n).split(b"\n")[:-1]
+        return [b"\n".join(lines[0::2]) + b"\n", b"\n".join(lines[1::2]) + b"\n"], [(0, t) for t in w["thresholds"]]
     if w["kind"] != "batch":
         return [make_text(w, seed_offset, n)], [(0, t) for t in w["thresholds"]]
     from new_fgssjoin_b200 import datagen
@@ -181,6 +187,9 @@ def cpu_sample(w, jobs):
 def oracle_sets(w, texts, sample):
     """Memory-order records of the sampled files, tokenized by the oracle."""
     from oracle import oracle as O
+    if w["kind"] == "rs":
+        (_, rp, rl, rt), (_, sp, sl, stk), nt = O.tokenize_dual(texts[0], texts[1], **tok_opts(w))
+        return {0: (rp, rl, rt, nt), 1: (sp, sl, stk, nt)}
     mem = {}
     for ti, _ in sample:
         if ti not in mem:
@@ -204,13 +213,17 @@ def cpu_reference(w, jobs, mem, steps, warmup):
         c = 0
         for ti, t in sample:
             mpos, mlen, mtok, nt = mem[ti]
-            _, st = O.join(mpos, mlen, mtok, nt, t, threads=threads)
+            if w["kind"] == "rs":  # R-S join of file 0 (R) with file 1 (S)
+                _, st = O.rsjoin(mem[0][:3], mem[1][:3], nt, t, threads=threads)
+            else:
+                _, st = O.join(mpos, mlen, mtok, nt, t, threads=threads)
             c += st["candidates"]
         dt = time.perf_counter() - t0
         if it >= warmup:
             times.append(dt)
             cands.append(c)
-    recs = sum(len(mem[ti][1]) for ti in {ti for ti, _ in sample})
+    recs = sum(len(m[1]) for m in mem.values()) if w["kind"] == "rs" else \
+        sum(len(mem[ti][1]) for ti in {ti for ti, _ in sample})
     note = ("%d of %d joins (%d records), oracle restatement, OpenMP, %d threads"
             % (len(sample), len(jobs), recs, threads))
     return float(np.sum(cands) / np.sum(times)), float(np.mean(times) * 1000.0), threads, note
@@ -315,13 +328,15 @@ def main():
 
     # ---- inputs (untimed): text -> GPU tokenizer -> device-resident sets + pinned host copies
     sets, d_arrays, host_sets = [], [], []
-    for text in texts:
-        s = ctx.tokenize(text, **to)
+    tokenized = list(ctx.tokenize_dual(texts[0], texts[1], **to)) if w["kind"] == "rs" else \
+        [ctx.tokenize(text, **to) for text in texts]
+    tune_union = ctx.tokenize(texts[0] + texts[1], **to) if w["kind"] == "rs" and not args.no_tune else None
+    for s in tokenized:
         sets.append(s)
         d_arrays.append([torch.from_numpy(a.view(np.int32)).to(dev) for a in (s.id, s.pos, s.len, s.tokens)])
         pinned = [torch.from_numpy(a.view(np.int32)).pin_memory() for a in (s.id, s.pos, s.len, s.tokens)]
         host_sets.append(F.Sets(*(p.numpy().view(np.uint32) for p in pinned), n_terms=s.n_terms))
-    del texts
+    del texts, tokenized
 
     def dev_view(ti):
         v = _View()
@@ -352,12 +367,18 @@ def main():
     tuned = {}
     if not args.no_tune:
         for t in t_list:
+            if w["kind"] == "rs":  # the R-S join runs on the union of R and S: tune on a self-join that size
+                tuned[str(t)] = ctx.autotune(tune_union, t, reps=1)
+                continue
             ti = max((j for j in jobs if j[1] == t), key=lambda j: sets[j[0]].n_tokens)[0]
             tuned[str(t)] = ctx.autotune(dev_view(ti), t, reps=1)
+    tune_union = None
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
 
     def step_batched(view_fn):
+        if w["kind"] == "rs":
+            return [ctx.rsjoin(view_fn(0), view_fn(1), t, method="batched", use_model=use_model) for t in ts]
         return ctx.selfjoin_batch([view_fn(ti) for ti, _ in jobs], ts, method="batched", use_model=use_model)
 
     def step_plain(view_fn, per_join_ms=None):
@@ -368,7 +389,10 @@ def main():
                 a = torch.cuda.Event(enable_timing=True)
                 b = torch.cuda.Event(enable_timing=True)
                 a.record(stream)
-            outs += ctx.selfjoin_batch([view_fn(ti)], [t], method="plain")
+            if w["kind"] == "rs":
+                outs.append(ctx.rsjoin(view_fn(0), view_fn(1), t, method="plain"))
+            else:
+                outs += ctx.selfjoin_batch([view_fn(ti)], [t], method="plain")
             if per_join_ms is not None:
                 b.record(stream)
                 b.synchronize()
@@ -416,7 +440,9 @@ def main():
     cands = sum(o.stats["candidates"] for o in bat_out)
     # e2e: host (pinned) inputs, H2D + join + D2H of the pairs inside the timed region
     e2e_ms, e2e_out, _ = timed(lambda: step_batched(host_view), args.steps, 1, "e2e_step")
-    h2d = sum(sum(a.nbytes for a in (sets[ti].id, sets[ti].pos, sets[ti].len, sets[ti].tokens)) for ti, _ in jobs)
+    files_per_join = [0, 1] if w["kind"] == "rs" else None
+    h2d = sum(sum(sum(a.nbytes for a in (sets[k].id, sets[k].pos, sets[k].len, sets[k].tokens))
+                  for k in (files_per_join or [ti])) for ti, _ in jobs)
     d2h = sum(len(o) * 24 for o in e2e_out)
     same_e2e = all(np.array_equal(a.q, b.q) and np.array_equal(a.s, b.s) for a, b in zip(e2e_out, plain_out))
 
@@ -453,7 +479,9 @@ def main():
 
     # roofline of the fused filter+verify kernel (one launch per step covers every join of the step)
     last = bat_stats[-1]
-    kern_ms = float(np.mean([s[0]["ms_probe"] for s in bat_stats]))
+    # (an R-S step is one call per threshold; a batched self-join step is one call for all its joins)
+    kern_ms = float(np.mean([sum(x["ms_probe"] for x in s) if w["kind"] == "rs" else s[0]["ms_probe"]
+                             for s in bat_stats]))
     P = sum(s["probe_tokens"] for s in last)
     W = sum(s["window_entries"] for s in last)
     M = sum(s["merged_tokens"] for s in last)
@@ -461,18 +489,20 @@ def main():
     alg_bytes = 12 * P + 8 * W + 4 * M + 12 * R
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (kern_ms * 1e-3) / 1e9 if kern_ms > 0 else 0.0
-    launches = int(np.mean([s[0]["launches"] for s in bat_stats]))
+    launches = int(np.mean([sum(x["launches"] for x in s) if w["kind"] == "rs" else s[0]["launches"]
+                            for s in bat_stats]))
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         # the same records the GPU joined (the GPU tokenizer's output equals the oracle's)
-        mem = {ti: (sets[ti].pos, sets[ti].len, sets[ti].tokens, sets[ti].n_terms) for ti, _ in cpu_sample(w, jobs)}
+        mem = {ti: (sets[ti].pos, sets[ti].len, sets[ti].tokens, sets[ti].n_terms)
+               for ti in (range(len(sets)) if w["kind"] == "rs" else {ti for ti, _ in cpu_sample(w, jobs)})}
         v, ms, threads, note = cpu_reference(w, jobs, mem, 1, 0)
         cpu = {"value": v, "unit": "candidates/s", "cores": threads, "kind": "port", "sample": note}
 
     if rank == 0:
         per_step = bat_ms / args.steps
-        uniq = sorted({ti for ti, _ in jobs})
+        uniq = range(len(sets)) if w["kind"] == "rs" else sorted({ti for ti, _ in jobs})
         line = {
             "metric": METRIC,
             "value": ws * cands / (per_step * 1e-3), "unit": "candidates/s", "n_gpus": ws, "steps": args.steps,

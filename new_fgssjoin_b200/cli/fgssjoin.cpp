@@ -9,7 +9,9 @@
 // Options of the second form: --pad (pad q-grams), --distinct (one token per
 // distinct gram instead of gram + occurrence), --kmer (canonical k-mers, k = q),
 // --method plain|batched, --bounds reference|exact, --write-bin <path> (also
-// write the tokenized .bin and .bin.loc), --device <n>.
+// write the tokenized .bin and .bin.loc), --device <n>, and -s <text>: an R-S
+// join of the -f file (R) with this one (S) over one vocabulary, printing
+// "id_in_R id_in_S similarity" (no reference counterpart).
 // stdout: "id id similarity" per pair (block.cu:193); stderr: the reference's
 // counters and timers (fgssjoin_cli.cu:55-65,92,108; block.cu:209-212).
 #include <stdio.h>
@@ -34,11 +36,23 @@ static int die(fgss_ctx* ctx, fgss_status st, const char* what) {
     return 1;
 }
 
+static bool read_file(const std::string& path, std::vector<char>& buf) {
+    FILE* f = fopen(path.c_str(), "rb");
+    if (!f) return false;
+    fseek(f, 0, SEEK_END);
+    long sz = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    buf.assign((size_t)(sz > 0 ? sz : 0), 0);
+    const bool ok = sz <= 0 || fread(buf.data(), 1, (size_t)sz, f) == (size_t)sz;
+    fclose(f);
+    return ok;
+}
+
 static void usage(const char* argv0) {
     fprintf(stdout,
             "Usage:\n"
             "  %s <ppjoin bin file> <threshold> [verbose|debug]\n"
-            "  %s -f <text file> -q <q> -t <threshold> [--pad] [--distinct] [--kmer]\n"
+            "  %s -f <text file> [-s <second text file>] -q <q> -t <threshold> [--pad] [--distinct] [--kmer]\n"
             "     [--method plain|batched] [--bounds reference|exact] [--write-bin <path>] [--device <n>]\n",
             argv0, argv0);
 }
@@ -48,7 +62,7 @@ int main(int argc, char** argv) {
         usage(argv[0]);
         return 1;
     }
-    std::string bin_path, text_path, write_bin;
+    std::string bin_path, text_path, second_path, write_bin;
     float threshold = 0.f;
     int q = 3, pad = 0, suffix = 1, kmer = 0, method = FGSS_METHOD_PLAIN, bounds = FGSS_BOUNDS_REFERENCE;
     int device = 0;
@@ -64,6 +78,7 @@ int main(int argc, char** argv) {
                 return argv[++i];
             };
             if (a == "-f") text_path = next("-f");
+            else if (a == "-s") second_path = next("-s");
             else if (a == "-q") q = atoi(next("-q"));
             else if (a == "-t") threshold = (float)atof(next("-t"));
             else if (a == "--pad") pad = 1;
@@ -92,9 +107,11 @@ int main(int argc, char** argv) {
         }
     }
     const std::string& in_path = bin_path.empty() ? text_path : bin_path;
-    if (access(in_path.c_str(), F_OK) == -1) {
-        fprintf(stderr, "File \"%s\" does not exist.\n", in_path.c_str());
-        return 1;
+    for (const std::string* pth : std::vector<const std::string*>{&in_path, &second_path}) {
+        if (!pth->empty() && access(pth->c_str(), F_OK) == -1) {
+            fprintf(stderr, "File \"%s\" does not exist.\n", pth->c_str());
+            return 1;
+        }
     }
     if (threshold <= 0.0f || threshold >= 1.0) {
         fprintf(stderr, "Threshold must be a float in the range (0.0..1.0).\n");
@@ -112,6 +129,45 @@ int main(int argc, char** argv) {
     fgss_status st = fgss_create(&ctx, &o);
     if (st != FGSS_OK) return die(nullptr, st, "fgss_create");
 
+    fgss_tok_opts to;
+    fgss_tok_opts_default(&to);
+    to.q = q;
+    to.mode = kmer ? FGSS_TOK_KMER : FGSS_TOK_QGRAM;
+    to.pad = pad;
+    to.suffix = suffix;
+    if (!second_path.empty()) {
+        // R-S join of the -f text (R) with the -s text (S)
+        std::vector<char> tr, ts;
+        if (!read_file(text_path, tr) || !read_file(second_path, ts)) return die(ctx, FGSS_ERR_IO, "read");
+        fgss_sets r, s2;
+        st = fgss_tokenize_dual(ctx, tr.data(), tr.size(), ts.data(), ts.size(), &to, &r, &s2);
+        if (st != FGSS_OK) return die(ctx, st, "fgss_tokenize_dual");
+        fprintf(stderr, "# Records: %llu + %llu\n# Terms: %u\n", (unsigned long long)r.n_sets,
+                (unsigned long long)s2.n_sets, r.n_terms);
+        fprintf(stderr, "=== BEGIN JOIN (TIMER STARTED) ===\n");
+        double t0 = now_us();
+        fgss_sets_view vr = fgss_sets_view_of(&r), vs = fgss_sets_view_of(&s2);
+        fgss_join_opts jo;
+        fgss_join_opts_default(&jo);
+        jo.threshold = threshold;
+        jo.method = method;
+        jo.bounds = bounds;
+        fgss_pairs pairs;
+        fgss_stats stats;
+        st = fgss_rsjoin(ctx, &vr, &vs, &jo, &pairs, &stats);
+        if (st != FGSS_OK) return die(ctx, st, "fgss_rsjoin");
+        fgss_pairs_print(&pairs, stdout);
+        fprintf(stderr, "# Candidates: %llu\n", (unsigned long long)stats.candidates);
+        fprintf(stderr, "# Intersections: %llu\n", (unsigned long long)stats.intersections);
+        fprintf(stderr, "# Results: %llu\n", (unsigned long long)stats.results);
+        fprintf(stderr, "===  END JOIN (TIMER STOPPED)  ===\n");
+        fprintf(stderr, "Total Running Time: %g s\n", (now_us() - t0) / 1e6);
+        fgss_pairs_free(&pairs);
+        fgss_sets_free(&r);
+        fgss_sets_free(&s2);
+        fgss_destroy(ctx);
+        return 0;
+    }
     fprintf(stderr, "... LOADING DATASET ...\n");
     fgss_sets sets;
     memset(&sets, 0, sizeof sets);
@@ -119,20 +175,8 @@ int main(int argc, char** argv) {
         st = fgss_load_bin(bin_path.c_str(), &sets);
         if (st != FGSS_OK) return die(ctx, st, "fgss_load_bin");
     } else {
-        FILE* f = fopen(text_path.c_str(), "rb");
-        if (!f) return die(ctx, FGSS_ERR_IO, "open");
-        fseek(f, 0, SEEK_END);
-        long sz = ftell(f);
-        fseek(f, 0, SEEK_SET);
-        std::vector<char> buf((size_t)(sz > 0 ? sz : 0));
-        if (sz > 0 && fread(buf.data(), 1, (size_t)sz, f) != (size_t)sz) return die(ctx, FGSS_ERR_IO, "read");
-        fclose(f);
-        fgss_tok_opts to;
-        fgss_tok_opts_default(&to);
-        to.q = q;
-        to.mode = kmer ? FGSS_TOK_KMER : FGSS_TOK_QGRAM;
-        to.pad = pad;
-        to.suffix = suffix;
+        std::vector<char> buf;
+        if (!read_file(text_path, buf)) return die(ctx, FGSS_ERR_IO, "read");
         st = fgss_tokenize(ctx, buf.data(), buf.size(), &to, &sets);
         if (st != FGSS_OK) return die(ctx, st, "fgss_tokenize");
         if (!write_bin.empty()) {

@@ -226,6 +226,25 @@ def bounds_table(t, maxlen):
             np.array([L.orc_max_size(ft, int(i)) for i in n], np.uint32))
 
 
+def tokenize_dual(text_r, text_s, **tok):
+    """Oracle tokenization of R's text then S's text as one input (one shared
+    vocabulary), split into the two sides the way fgss_tokenize_dual splits
+    them: ((id, pos, len, tokens) of R, the same of S, n_terms), MEMORY order,
+    ids counting the non-empty lines of each side's own text."""
+    if text_r and not text_r.endswith(b"\n"):
+        text_r = text_r + b"\n"
+    nr = sum(1 for x in text_r.split(b"\n") if x)
+    ids, lens, tok_, loc, nt = tokenize(text_r + text_s, **tok)
+    mid, mpos, mlen, mtok = file_to_memory(ids, lens, tok_)
+
+    def side(mask, shift):
+        ln = mlen[mask]
+        t = np.concatenate([mtok[p:p + n] for p, n in zip(mpos[mask], ln)]) if len(ln) else np.zeros(0, np.uint32)
+        p = np.concatenate([[0], np.cumsum(ln[:-1])]).astype(np.uint32) if len(ln) else np.zeros(0, np.uint32)
+        return mid[mask] - shift, p, ln, t.astype(np.uint32)
+    return side(mid <= nr, 0), side(mid > nr, nr), nt
+
+
 def rs_union(r_len, s_len):
     """Memory order of the union of two record sets (each in memory order):
     descending size, then R before S, then the index within its side.

@@ -1,0 +1,59 @@
+"""The fgssjoin command line (both argument forms, and the R-S form) on a B200."""
+import json
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from new_fgssjoin_b200 import datagen
+from oracle import oracle as O
+from rs_util import split_titles, oracle_dual
+
+pytestmark = pytest.mark.gpu
+
+CLI = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "new_fgssjoin_b200", "_lib",
+                   "fgssjoin")
+
+
+def _run(args):
+    p = subprocess.run([CLI] + args, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    counters = {k: int(v) for k, v in re.findall(r"# (Candidates|Intersections|Results): (\d+)", p.stderr)}
+    return [x for x in p.stdout.splitlines() if x], counters
+
+
+def test_reference_argument_form_prints_the_golden_pairs():
+    for t in ("0.5", "0.7", "0.9"):
+        lines, _ = _run([os.path.join(GOLDEN, "small.txt.3gram.bin"), t])
+        assert sorted(lines) == json.load(open(os.path.join(GOLDEN, "small_pairs.json")))[t]
+
+
+def test_text_form_matches_oracle(tmp_path):
+    text = datagen.titles(3000, seed=21)
+    f = tmp_path / "titles.txt"
+    f.write_bytes(text)
+    ids, lens, tok, loc, nt = O.tokenize(text, q=3, pad=True, suffix=False)
+    mid, mpos, mlen, mtok = O.file_to_memory(ids, lens, tok)
+    ref, st = O.join(mpos, mlen, mtok, nt, 0.8)
+    want = ["%d %d %f" % (mid[q], mid[s], x) for q, s, x in zip(ref["q"], ref["s"], ref["sim"])]
+    for extra in ([], ["--method", "batched"]):
+        lines, cnt = _run(["-f", str(f), "-q", "3", "-t", "0.8", "--pad", "--distinct"] + extra)
+        assert lines == want
+        assert cnt == {"Candidates": st["candidates"], "Intersections": st["intersections"],
+                       "Results": st["results"]}
+
+
+def test_rs_form_matches_oracle(tmp_path):
+    tr, ts = split_titles(3000, 22)
+    (tmp_path / "r.txt").write_bytes(tr)
+    (tmp_path / "s.txt").write_bytes(ts)
+    (rid, rp, rl, rt), (sid, sp, sl, stk), nt = oracle_dual(tr, ts, q=3, pad=True, suffix=False)
+    ref, st = O.rsjoin((rp, rl, rt), (sp, sl, stk), nt, 0.7)
+    want = ["%d %d %f" % (rid[r], sid[s], x) for r, s, x in zip(ref["r"], ref["s"], ref["sim"])]
+    lines, cnt = _run(["-f", str(tmp_path / "r.txt"), "-s", str(tmp_path / "s.txt"), "-q", "3", "-t", "0.7",
+                       "--pad", "--distinct", "--method", "batched"])
+    assert len(want) > 0 and lines == want
+    assert cnt["Results"] == st["results"] and cnt["Candidates"] == st["candidates"]
