@@ -231,6 +231,7 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         uint32_t* fcost = c.devT<uint32_t>(J.pfx("fcost"), n + 1);
         uint32_t* poff = c.devT<uint32_t>(J.pfx("poff"), n + 1);
         uint2* win = c.devT<uint2>(J.pfx("win"), J.in.n_tokens + 1);
+        uint32_t* wpre = c.devT<uint32_t>(J.pfx("wpre"), J.in.n_tokens + 1);
         uint32_t* wtot = c.devT<uint32_t>(J.pfx("wtot"), n + 1);
         uint32_t* pred = c.devT<uint32_t>(J.pfx("pred"), n + 1);
         pre[i] = c.devT<uint64_t>(J.pfx("cpre"), n + 1);
@@ -240,6 +241,7 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         uint32_t* cbuf = c.devT<uint32_t>(J.pfx("cbuf"), cbuf_cap);
         hf[i].poff = poff;
         hf[i].win = win;
+        hf[i].wpre = wpre;
         hf[i].smin = J.lut.smin;
         hf[i].meta = meta;
         hf[i].qchunk = qchunk;
@@ -250,7 +252,7 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         exclusive_scan<uint32_t>(c, J.pcnt, poff, n, nullptr, (uint32_t*)nullptr, J.pfx("scan.p").c_str());
         unsigned long long* cused = reinterpret_cast<unsigned long long*>(J.status + 4);
         FGSS_CK(cudaMemsetAsync(cused, 0, 8, c.stream));
-        k_windows<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wtot, meta);
+        k_windows<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wpre, wtot, meta);
         FGSS_LAUNCH_CK();
         k_chunks<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wtot, cap_entries,
                                                                             qchunk, cbuf, cbuf_cap, cused);

@@ -70,10 +70,12 @@ struct FusedLayout {
     static_assert(off_bm % 16 == 0, "the membership words are cleared with 16-byte stores");
 };
 
-// Window of every probe token: warp per query.  win[poff[q] + j] = (lo, hi);
-// wtot[q] = sum of the window sizes.
+// Window of every probe token: warp per query.  win[poff[q] + j] = (lo, hi),
+// wpre[poff[q] + j] = entries in the query's windows before window j,
+// wtot[q] = sum of the window sizes (also meta[q].w).
 static __global__ void k_windows(JoinArgs a, const uint32_t* __restrict__ poff, uint2* __restrict__ win,
-                                 uint32_t* __restrict__ wtot, uint4* __restrict__ meta) {
+                                 uint32_t* __restrict__ wpre, uint32_t* __restrict__ wtot,
+                                 uint4* __restrict__ meta) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t lane = lane_id();
     const bool unsorted = (*a.status & ST_UNSORTED) != 0;
@@ -84,22 +86,30 @@ static __global__ void k_windows(JoinArgs a, const uint32_t* __restrict__ poff, 
         const uint32_t send = unsorted ? a.n : (lq <= 65535u ? a.send[lq] : 0);
         const uint32_t* qt = a.tok + a.pos[q];
         const uint32_t o = poff[q];
-        uint32_t tot = 0;
-        for (uint32_t j = lane; j < qp; j += 32) {
-            const uint32_t w = __ldg(qt + j);
-            const uint32_t b = __ldg(a.list_off + w), e = __ldg(a.list_off + w + 1);
-            uint32_t lo = e, hi = e;
-            if (send > q + 1) {
-                lo = lower_bound_u32(a.ent_s, b, e, q + 1);
-                hi = unsorted ? e : lower_bound_u32(a.ent_s, lo, e, send);
+        uint32_t tot = 0;  // running total of the windows before this round (same in every lane)
+        for (uint32_t j0 = 0; j0 < qp; j0 += 32) {
+            const uint32_t j = j0 + lane;
+            uint32_t lo = 0, hi = 0;
+            if (j < qp) {
+                const uint32_t w = __ldg(qt + j);
+                const uint32_t b = __ldg(a.list_off + w), e = __ldg(a.list_off + w + 1);
+                lo = e;
+                hi = e;
+                if (send > q + 1) {
+                    lo = lower_bound_u32(a.ent_s, b, e, q + 1);
+                    hi = unsorted ? e : lower_bound_u32(a.ent_s, lo, e, send);
+                }
             }
-            win[o + j] = make_uint2(lo, hi);
-            tot += hi - lo;
+            const uint32_t incl = warp_incl_scan(hi - lo);
+            if (j < qp) {
+                win[o + j] = make_uint2(lo, hi);
+                wpre[o + j] = tot + incl - (hi - lo);
+            }
+            tot += __shfl_sync(kFull, incl, 31);
         }
-        tot = warp_sum(tot);
         if (lane == 0) {
             wtot[q] = tot;
-            meta[q] = make_uint4(a.pos[q], lq, lq <= 65535u ? a.index[lq] : 0u, 0u);
+            meta[q] = make_uint4(a.pos[q], lq, lq <= 65535u ? a.index[lq] : 0u, tot);
         }
     }
 }
@@ -154,7 +164,8 @@ struct FusedArgs {
     const uint32_t* poff;    // per query: first probe window
     const uint2* win;
     const uint4* smin;       // per length sum S: (cand_min, inter_min, need, 0)
-    const uint4* meta;       // per record: (pos, len, index prefix, 0)
+    const uint4* meta;       // per record: (pos, len, index prefix, window entries)
+    const uint32_t* wpre;    // per probe window: entries of the query's earlier windows
     const uint2* qchunk;     // per query: (first boundary in cbuf, number of chunks)
     const uint32_t* cbuf;    // chunk boundaries: per inner boundary, first entry of each probe window
 };
@@ -279,10 +290,18 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
         if (staged) qtok[j] = x;
         bm_insert(bm, qmode, x);
     }
+    // one chunk that fits the slot table (the common case): the pre-pass's
+    // window prefix is used as is, with no block-wide scan
+    const bool one_chunk = nch == 1 && qm.w <= Lay::cap;
+    const uint32_t* qpre = fa.wpre + fa.poff[q];
     for (uint32_t j = tid; j < qp; j += NT) {
         const uint2 w = qwin[j];
         wlo[j] = w.x;
         whi[j] = w.y;
+        if (one_chunk) {
+            clo[j] = w.x;
+            wpre[j] = qpre[j];
+        }
     }
     if (tid == 0) {
         s_cand = 0;
@@ -305,7 +324,14 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
             const uint32_t sp = s_sp;
             if (sp == 0) break;
             const uint32_t ra = s_sa[sp - 1], rb = s_sb[sp - 1], tag = s_sc[sp - 1];
-            {
+            if (one_chunk) {
+                if (tid == 0) {
+                    wpre[qp] = qm.w;
+                    s_L = qm.w;
+                    s_nocc = 0;
+                    s_next = 0;
+                }
+            } else {
                 constexpr uint32_t PER = (Lay::PC + NT - 1) / NT;
                 const uint32_t b0 = tid * PER;
                 uint32_t loc[PER];
