@@ -440,9 +440,14 @@ def main():
     cands = sum(o.stats["candidates"] for o in bat_out)
     # e2e: host (pinned) inputs, H2D + join + D2H of the pairs inside the timed region
     e2e_ms, e2e_out, _ = timed(lambda: step_batched(host_view), args.steps, 1, "e2e_step")
-    files_per_join = [0, 1] if w["kind"] == "rs" else None
-    h2d = sum(sum(sum(a.nbytes for a in (sets[k].id, sets[k].pos, sets[k].len, sets[k].tokens))
-                  for k in (files_per_join or [ti])) for ti, _ in jobs)
+    # bytes copied to the device per step: an R-S join copies both files per call; the joins of one
+    # batched call that share host arrays copy them once
+    def set_bytes(k):
+        return sum(a.nbytes for a in (sets[k].id, sets[k].pos, sets[k].len, sets[k].tokens))
+    if w["kind"] == "rs":
+        h2d = len(jobs) * (set_bytes(0) + set_bytes(1))
+    else:
+        h2d = sum(set_bytes(k) for k in {ti for ti, _ in jobs})
     d2h = sum(len(o) * 24 for o in e2e_out)
     same_e2e = all(np.array_equal(a.q, b.q) and np.array_equal(a.s, b.s) for a, b in zip(e2e_out, plain_out))
 

@@ -303,7 +303,20 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
         for (int i = 0; i < n; i++) {
             js[i].reset(new JoinState());
             if (g) js[i]->ns = g->ns;
-            join_setup(c, *js[i], sets[i], opts[i], i, false);
+            fgss_sets_view v = sets[i];
+            if (!v.on_device) {
+                // the same host arrays as an earlier join of the batch: copied to the device once
+                for (int j = 0; j < i; j++) {
+                    const fgss_sets_view& w = sets[j];
+                    if (!w.on_device && w.id == v.id && w.pos == v.pos && w.len == v.len && w.tokens == v.tokens &&
+                        w.n_sets == v.n_sets && w.n_tokens == v.n_tokens) {
+                        v = js[j]->in;
+                        v.n_terms = sets[i].n_terms;
+                        break;
+                    }
+                }
+            }
+            join_setup(c, *js[i], v, opts[i], i, false);
         }
         c.sync();  // one wait for the whole batch's input validation
         for (int i = 0; i < n; i++) join_check_input(c, *js[i]);

@@ -169,6 +169,17 @@ def test_batch_of_joins_equals_single_joins(ctx):
         _check_same(got, ref, st)
 
 
+def test_batch_sharing_host_arrays(ctx, titles_sets):
+    """Joins of one batched call on the same host arrays (copied to the device once)."""
+    s = titles_sets
+    ts = [0.6, 0.9, 0.75]
+    for method in ("batched", "plain"):
+        outs = ctx.selfjoin_batch([s, s, s], ts, method=method)
+        for t, got in zip(ts, outs):
+            ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, t)
+            _check_same(got, ref, st)
+
+
 def test_long_records_take_the_heavy_path(ctx):
     """Records longer than the shared-memory caps go through the global accumulator."""
     rng = np.random.default_rng(4)
