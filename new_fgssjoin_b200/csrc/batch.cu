@@ -98,9 +98,10 @@ __global__ void k_permute_items(const uint4* __restrict__ items, const uint32_t*
 template <int NT, int HLOG, int RT>
 static int resident_ctas(Ctx& c) {
     int occ = 0;
-    FGSS_CK(cudaFuncSetAttribute(k_fused<NT, HLOG, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    FGSS_CK(cudaFuncSetAttribute(k_fused<NT, HLOG, RT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)FusedLayout<HLOG>::bytes));
-    FGSS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused<NT, HLOG, RT>, NT, FusedLayout<HLOG>::bytes));
+    FGSS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused<NT, HLOG, RT, false>, NT,
+                                                          FusedLayout<HLOG>::bytes));
     return std::max(occ, 1) * c.num_sms;
 }
 
@@ -121,21 +122,22 @@ int fused_resident_ctas(Ctx& c, const TuneEntry& te) {
     return resident_ctas<64, 9, 768>(c);
 }
 
-template <int NT, int HLOG, int RT>
+template <int NT, int HLOG, int RT, bool SIDED>
 static void launch_fused(Ctx& c, const JoinArgs* d_args, const FusedArgs* d_fargs, const uint4* items,
                          uint32_t n_items, uint32_t* counter, int ctas_per_sm) {
     static bool attr = false;
     const size_t smem = FusedLayout<HLOG>::bytes;
     if (!attr) {
-        FGSS_CK(cudaFuncSetAttribute(k_fused<NT, HLOG, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        FGSS_CK(cudaFuncSetAttribute(k_fused<NT, HLOG, RT, SIDED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
         attr = true;
     }
     int occ = 0;
-    FGSS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused<NT, HLOG, RT>, NT, smem));
+    FGSS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused<NT, HLOG, RT, SIDED>, NT, smem));
     if (occ < 1) occ = 1;
     const int per = ctas_per_sm > 0 ? std::min(occ, ctas_per_sm) : occ;
     const unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)per * c.num_sms, std::max<uint32_t>(n_items, 1));
-    k_fused<NT, HLOG, RT><<<grid, NT, smem, c.stream>>>(d_args, d_fargs, items, n_items, counter);
+    k_fused<NT, HLOG, RT, SIDED><<<grid, NT, smem, c.stream>>>(d_args, d_fargs, items, n_items, counter);
     FGSS_LAUNCH_CK();
 }
 
@@ -146,12 +148,14 @@ extern const int kFusedShapes[][3] = {{32, 8, 1024},  {32, 9, 1024},  {64, 9, 10
                                       {128, 11, 768}, {256, 11, 768}};
 extern const int kNumFusedShapes = 10;
 
+// sided: the batch is an R-S join (its records carry a side byte)
 void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const FusedArgs* d_fargs, const uint4* items,
-                  uint32_t n_items, uint32_t* counter) {
-#define FGSS_F(NT, HL, RT)                                                                     \
-    if (te.threads == NT && te.hash_log2 == HL && te.regs_rt == RT) {                          \
-        launch_fused<NT, HL, RT>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm); \
-        return;                                                                                \
+                  uint32_t n_items, uint32_t* counter, bool sided) {
+#define FGSS_F(NT, HL, RT)                                                                               \
+    if (te.threads == NT && te.hash_log2 == HL && te.regs_rt == RT) {                                    \
+        if (sided) launch_fused<NT, HL, RT, true>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm); \
+        else launch_fused<NT, HL, RT, false>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm);      \
+        return;                                                                                          \
     }
     FGSS_F(32, 8, 1024)
     FGSS_F(32, 9, 1024)
@@ -164,7 +168,8 @@ void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const Fus
     FGSS_F(128, 11, 768)
     FGSS_F(256, 11, 768)
 #undef FGSS_F
-    launch_fused<64, 9, 768>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm);
+    if (sided) launch_fused<64, 9, 768, true>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm);
+    else launch_fused<64, 9, 768, false>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm);
 }
 
 // Work-item cost of a query: exact window entries + a verification estimate.
@@ -286,9 +291,10 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         }
         uint64_t grand = 0;
         for (size_t i = 0; i < nj; i++) grand += htot[i];
-        // ~32 items per resident CTA over the whole batch, split by cost share and
-        // handed out longest first, so the dynamic queue ends with short items
-        const uint64_t want = (uint64_t)32 * fused_resident_ctas(c, te);
+        // ~256 items per resident CTA over the whole batch (a few queries per item at
+        // 100k records), split by cost share and handed out longest first, so the
+        // dynamic queue ends with short items
+        const uint64_t want = (uint64_t)256 * fused_resident_ctas(c, te);
         for (size_t i = 0; i < nj; i++) {
             const uint64_t n = joins[i]->in.n_sets;
             if (n == 0) continue;
@@ -366,7 +372,9 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
     // (inside a capture the events must be external record nodes to be timed at replay)
     const unsigned rec_flags = capture ? cudaEventRecordExternal : 0u;
     FGSS_CK(cudaEventRecordWithFlags(c.ev[4], c.stream, rec_flags));
-    if (nitems) fused_launch(c, te, d_args, d_fargs, items, (uint32_t)nitems, counter);
+    bool sided = false;
+    for (size_t i = 0; i < nj; i++) sided |= joins[i]->args.side != nullptr;
+    if (nitems) fused_launch(c, te, d_args, d_fargs, items, (uint32_t)nitems, counter, sided);
     FGSS_CK(cudaEventRecordWithFlags(c.ev[5], c.stream, rec_flags));
     c.probe_timed = true;
     // heavy queries: one persistent launch per join.  Eagerly only when some

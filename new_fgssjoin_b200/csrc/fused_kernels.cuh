@@ -214,6 +214,27 @@ __device__ __forceinline__ void bm_insert(uint32_t* bm, uint32_t mode, uint32_t 
     atomicOr(&bm[b >> 5], 1u << (b & 31));
 }
 
+// The fused kernel's per-thread counters, 32-bit to keep registers free; they
+// are added to the join's 64-bit statistics when the CTA moves to another join
+// (or one of them passes 2^30) and at the end.
+struct FusedCounters {
+    uint32_t cand, inter, res, window, verified, merged;
+};
+
+// Warp-collective: adds the warp's counters to the join's statistics and clears them.
+__device__ __forceinline__ void flush_fused_counters(const JoinArgs& a, FusedCounters& c) {
+    const unsigned long long v[6] = {warp_sum((unsigned long long)c.cand), warp_sum((unsigned long long)c.inter),
+                                     warp_sum((unsigned long long)c.res), warp_sum((unsigned long long)c.window),
+                                     warp_sum((unsigned long long)c.verified), warp_sum((unsigned long long)c.merged)};
+    if (lane_id() == 0) {
+        const int idx[6] = {SS_CANDIDATES, SS_INTERSECTIONS, SS_RESULTS, SS_WINDOW, SS_VERIFIED, SS_MERGED};
+#pragma unroll
+        for (int i = 0; i < 6; i++)
+            if (v[i]) atomicAdd(&a.stats[idx[i]], v[i]);
+    }
+    c = {0, 0, 0, 0, 0, 0};
+}
+
 // One merge step: up to 8 source tokens from position k (two independent
 // 16-byte loads of the aligned chunks holding them; the second only when it
 // holds tokens of this record, so no load leaves the record's 16-byte blocks).
@@ -242,9 +263,10 @@ __device__ __forceinline__ uint32_t merge_step(const uint32_t* __restrict__ st, 
     return hits;
 }
 
-template <int NT, int HLOG>
+// SIDED: an R-S join (a.side set); self-joins use the instantiation without the side test.
+template <int NT, int HLOG, bool SIDED>
 __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, unsigned char* smem,
-                            CtaCounters& ctr) {
+                            FusedCounters& ctr) {
     using Lay = FusedLayout<HLOG>;
     unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem);
     uint16_t* occ = reinterpret_cast<uint16_t*>(smem + Lay::off_occ);
@@ -275,8 +297,8 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
         return;
     }
     const uint32_t qmode = a.n_terms <= Lay::BW * 32 ? QM_EXACT : (lq <= kQHashMax ? QM_HASH : QM_BLOOM);
-    const uint8_t* sidep = a.side;  // R-S join: skip sources on the query's own side
-    const uint8_t side_q = sidep ? __ldg(sidep + q) : 0;
+    const uint8_t* sidep = SIDED ? a.side : nullptr;  // R-S join: skip sources on the query's own side
+    const uint8_t side_q = SIDED ? __ldg(sidep + q) : 0;
     FGSS_PHASE_START();
     const uint32_t* qt = a.tok + qm.x;
     const bool staged = lq <= Lay::QC;
@@ -416,7 +438,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                     const uint32_t s = sv[u];
                     if (s == kEmpty) continue;
                     if (unsorted && !size_ok(a, lq, a.len[s])) continue;
-                    if (sidep && __ldg(sidep + s) == side_q) continue;
+                    if (SIDED && __ldg(sidep + s) == side_q) continue;
                     const uint32_t pos = jv[u];  // query position << 11 | source position
                     uint32_t h = hash_slot(s, hl);
                     bool done = false;
@@ -588,7 +610,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
 
 // RT = resident threads per SM the register budget is sized for (launch
 // bounds): 1024 caps a thread at 64 registers, 768 at 80, 512 at 128.
-template <int NT, int HLOG, int RT>
+template <int NT, int HLOG, int RT, bool SIDED>
 __global__ void __launch_bounds__(NT, RT / NT) k_fused(const JoinArgs* __restrict__ joins, const FusedArgs* __restrict__ fargs,
                                               const uint4* __restrict__ items, uint32_t n_items,
                                               uint32_t* item_counter) {
@@ -599,26 +621,30 @@ __global__ void __launch_bounds__(NT, RT / NT) k_fused(const JoinArgs* __restric
     for (uint32_t h = threadIdx.x; h < Lay::H; h += NT) slots[h] = kEmptySlot;
     for (uint32_t i = threadIdx.x; i < Lay::BW; i += NT) bm[i] = 0u;
     __syncthreads();
-    CtaCounters ctr = {0, 0, 0, 0, 0, 0, 0};
-    __shared__ uint32_t s_item;
+    FusedCounters ctr = {0, 0, 0, 0, 0, 0};
+    // work items are claimed one ahead: thread 0 claims the next item as the
+    // current one starts, so one barrier per item publishes it
+    __shared__ uint32_t s_item[2];
     uint32_t cur_join = 0xffffffffu;
-    for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(item_counter, 1u);
-        __syncthreads();
-        const uint32_t it = s_item;
-        __syncthreads();
+    if (threadIdx.x == 0) s_item[0] = atomicAdd(item_counter, 1u);
+    __syncthreads();
+    for (uint32_t r = 0;; r ^= 1u) {
+        const uint32_t it = s_item[r];
         if (it >= n_items) break;
+        if (threadIdx.x == 0) s_item[r ^ 1u] = atomicAdd(item_counter, 1u);
         const uint4 w = items[it];
         if (w.x != cur_join) {
-            if (cur_join != 0xffffffffu) flush_counters_warp(joins[cur_join], ctr);
-            ctr = {0, 0, 0, 0, 0, 0, 0};
+            if (cur_join != 0xffffffffu) flush_fused_counters(joins[cur_join], ctr);
             cur_join = w.x;
         }
         const JoinArgs& a = joins[w.x];
         const FusedArgs& fa = fargs[w.x];
-        for (uint32_t q = w.y; q < w.z; q++) fused_query<NT, HLOG>(a, fa, q, smem, ctr);
+        for (uint32_t q = w.y; q < w.z; q++) fused_query<NT, HLOG, SIDED>(a, fa, q, smem, ctr);
+        const uint32_t big = max(max(ctr.cand, ctr.window), max(ctr.merged, ctr.verified));
+        if (__any_sync(kFull, big > (1u << 30))) flush_fused_counters(a, ctr);
+        __syncthreads();
     }
-    if (cur_join != 0xffffffffu) flush_counters_warp(joins[cur_join], ctr);
+    if (cur_join != 0xffffffffu) flush_fused_counters(joins[cur_join], ctr);
 }
 
 }  // namespace fgss
