@@ -219,6 +219,21 @@ void fgss_pairs_free(fgss_pairs* p);
  * (block.cu:193).  Writes to the FILE* given as a void* (stdout if NULL). */
 fgss_status fgss_pairs_print(const fgss_pairs* p, void* file);
 
+enum { FGSS_OUT_TEXT = 0, FGSS_OUT_BINARY = 1 };
+
+/* Streaming self-join for result sets too large to hold: the join runs as
+ * n_shards query ranges of about equal work (records are in memory order, the
+ * work of a query grows with its size squared), and a host thread formats and
+ * writes each shard's pairs to `path` while the GPU joins the next one, so
+ * output overlaps compute and at most two shards' pairs are in host memory.
+ * FGSS_OUT_TEXT writes the reference's "%d %d %f\n" line per pair (block.cu:193,
+ * printed there inside the join); FGSS_OUT_BINARY writes uint32 id_q, uint32 id_s,
+ * float sim per pair.  Pairs come out sorted by (q, s) as with fgss_selfjoin.
+ * stats: summed over the shards.  opts as for fgss_selfjoin, without a query
+ * range, out_on_device or want_candidates. */
+fgss_status fgss_selfjoin_to_file(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_join_opts* opts,
+                                  const char* path, int format, int n_shards, fgss_stats* stats);
+
 /* ------------------------------------------------------------- autotuner */
 
 typedef struct fgss_tune_result {

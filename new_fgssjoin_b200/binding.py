@@ -17,7 +17,7 @@ EXPORTED_SYMBOLS = [
     "fgss_load_bin", "fgss_write_bin", "fgss_sets_free", "fgss_sets_view_of",
     "fgss_tok_opts_default", "fgss_tokenize", "fgss_tokenize_dual",
     "fgss_join_opts_default", "fgss_selfjoin", "fgss_selfjoin_batch", "fgss_rsjoin", "fgss_pairs_free",
-    "fgss_pairs_print",
+    "fgss_pairs_print", "fgss_selfjoin_to_file",
     "fgss_model_train", "fgss_model_save", "fgss_model_load", "fgss_model_grad", "fgss_model_num_params",
     "fgss_autotune", "fgss_bounds_table", "fgss_dev_exclusive_scan_u32", "fgss_dev_sort_pairs_u64",
     "fgss_dev_exclusive_scan_u32_noalloc",
@@ -115,6 +115,8 @@ def load_library():
     L.fgss_tokenize_dual.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_char_p,
                                      ctypes.c_uint64, P(_TokOpts), P(_Sets), P(_Sets)]
     L.fgss_rsjoin.argtypes = [ctypes.c_void_p, P(_View), P(_View), P(_JoinOpts), P(_Pairs), P(_Stats)]
+    L.fgss_selfjoin_to_file.argtypes = [ctypes.c_void_p, P(_View), P(_JoinOpts), ctypes.c_char_p, ctypes.c_int,
+                                        ctypes.c_int, P(_Stats)]
     L.fgss_pairs_free.argtypes = [P(_Pairs)]
     L.fgss_model_train.argtypes = [ctypes.c_void_p, P(_View), P(ctypes.c_float), ctypes.c_int, ctypes.c_int,
                                    ctypes.c_float, ctypes.c_uint64, P(ctypes.c_float)]
@@ -385,6 +387,19 @@ class Context:
                                  ctypes.byref(st))
         _check(self._L, self._ctx, rc)
         return self._collect(p, st, False)
+
+    def selfjoin_to_file(self, sets, threshold, path, fmt="text", shards=4, method="batched", bounds="reference",
+                         use_model=False):
+        """Streaming self-join (fgss_selfjoin_to_file): the pairs go to ``path`` as the
+        reference's text lines (fmt "text") or 12-byte binary records (fmt "binary")
+        while the GPU joins the next of ``shards`` query ranges; returns the stats."""
+        v = sets.view() if isinstance(sets, Sets) else sets
+        o = self._opts(threshold, method, bounds, False, use_model)
+        st = _Stats()
+        rc = self._L.fgss_selfjoin_to_file(self._ctx, ctypes.byref(v), ctypes.byref(o), os.fsencode(path),
+                                           {"text": 0, "binary": 1}[fmt], int(shards), ctypes.byref(st))
+        _check(self._L, self._ctx, rc)
+        return _stats_dict(st)
 
     def selfjoin_batch(self, sets_list, thresholds, method="batched", bounds="reference", use_model=False,
                        result_capacity=0):

@@ -9,9 +9,11 @@
 // Options of the second form: --pad (pad q-grams), --distinct (one token per
 // distinct gram instead of gram + occurrence), --kmer (canonical k-mers, k = q),
 // --method plain|batched, --bounds reference|exact, --write-bin <path> (also
-// write the tokenized .bin and .bin.loc), --device <n>, and -s <text>: an R-S
+// write the tokenized .bin and .bin.loc), --device <n>, -s <text>: an R-S
 // join of the -f file (R) with this one (S) over one vocabulary, printing
-// "id_in_R id_in_S similarity" (no reference counterpart).
+// "id_in_R id_in_S similarity" (no reference counterpart), and
+// --out <path> [--shards K] [--binary]: the pairs streamed to a file while
+// the GPU joins the next of K query ranges (fgss_selfjoin_to_file).
 // stdout: "id id similarity" per pair (block.cu:193); stderr: the reference's
 // counters and timers (fgssjoin_cli.cu:55-65,92,108; block.cu:209-212).
 #include <stdio.h>
@@ -53,7 +55,8 @@ static void usage(const char* argv0) {
             "Usage:\n"
             "  %s <ppjoin bin file> <threshold> [verbose|debug]\n"
             "  %s -f <text file> [-s <second text file>] -q <q> -t <threshold> [--pad] [--distinct] [--kmer]\n"
-            "     [--method plain|batched] [--bounds reference|exact] [--write-bin <path>] [--device <n>]\n",
+            "     [--method plain|batched] [--bounds reference|exact] [--write-bin <path>] [--device <n>]\n"
+            "     [--out <path> [--shards <k>] [--binary]]\n",
             argv0, argv0);
 }
 
@@ -62,7 +65,8 @@ int main(int argc, char** argv) {
         usage(argv[0]);
         return 1;
     }
-    std::string bin_path, text_path, second_path, write_bin;
+    std::string bin_path, text_path, second_path, write_bin, out_path;
+    int shards = 4, out_binary = 0;
     float threshold = 0.f;
     int q = 3, pad = 0, suffix = 1, kmer = 0, method = FGSS_METHOD_PLAIN, bounds = FGSS_BOUNDS_REFERENCE;
     int device = 0;
@@ -79,6 +83,9 @@ int main(int argc, char** argv) {
             };
             if (a == "-f") text_path = next("-f");
             else if (a == "-s") second_path = next("-s");
+            else if (a == "--out") out_path = next("--out");
+            else if (a == "--shards") shards = atoi(next("--shards"));
+            else if (a == "--binary") out_binary = 1;
             else if (a == "-q") q = atoi(next("-q"));
             else if (a == "-t") threshold = (float)atof(next("-t"));
             else if (a == "--pad") pad = 1;
@@ -207,8 +214,16 @@ int main(int argc, char** argv) {
     jo.bounds = bounds;
     fgss_pairs pairs;
     fgss_stats stats;
-    st = fgss_selfjoin(ctx, &v, &jo, &pairs, &stats);
-    if (st != FGSS_OK) return die(ctx, st, "fgss_selfjoin");
+    memset(&pairs, 0, sizeof pairs);
+    if (!out_path.empty()) {
+        // streamed to the file shard by shard while the GPU joins the next shard
+        st = fgss_selfjoin_to_file(ctx, &v, &jo, out_path.c_str(), out_binary ? FGSS_OUT_BINARY : FGSS_OUT_TEXT,
+                                   shards > 0 ? shards : 1, &stats);
+        if (st != FGSS_OK) return die(ctx, st, "fgss_selfjoin_to_file");
+    } else {
+        st = fgss_selfjoin(ctx, &v, &jo, &pairs, &stats);
+        if (st != FGSS_OK) return die(ctx, st, "fgss_selfjoin");
+    }
     fprintf(stderr, "# Inverted Index Entries: %llu\n", (unsigned long long)stats.index_entries);
     double r0 = now_us();
     fgss_pairs_print(&pairs, stdout);

@@ -7,8 +7,12 @@
 #include <string.h>
 
 #include <algorithm>
+#include <condition_variable>
+#include <deque>
 #include <map>
 #include <memory>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "join.h"
@@ -685,6 +689,159 @@ fgss_status fgss_pairs_print(const fgss_pairs* p, void* file) {
     for (uint64_t i = 0; i < p->n; i++)
         fprintf(f, "%d %d %f\n", (int)p->id_q[i], (int)p->id_s[i], (double)p->sim[i]);  // block.cu:193
     return FGSS_OK;
+}
+
+fgss_status fgss_selfjoin_to_file(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_join_opts* opts,
+                                  const char* path, int format, int n_shards, fgss_stats* stats) {
+    if (!ctx || !sets || !opts || !path || n_shards < 1 || (format != FGSS_OUT_TEXT && format != FGSS_OUT_BINARY))
+        return FGSS_ERR_INVALID;
+    return guard(ctx, [&] {
+        Ctx& c = ctx->c;
+        FGSS_CK(cudaSetDevice(c.device));
+        if (opts->query_end > opts->query_begin) fail(FGSS_ERR_INVALID, "the shards cover every query");
+        if (opts->want_candidates || opts->out_on_device) fail(FGSS_ERR_INVALID, "pairs go to the file");
+        const uint64_t n = sets->n_sets;
+        // the inputs go to the device once; every shard joins against them
+        fgss_sets_view v = *sets;
+        std::vector<uint32_t> len(n);
+        if (!v.on_device) {
+            uint32_t* pos = c.devT<uint32_t>("wf.pos", n + 1);
+            uint32_t* ln = c.devT<uint32_t>("wf.len", n + 1);
+            uint32_t* tok = c.devT<uint32_t>("wf.tok", v.n_tokens + 1);
+            uint32_t* id = v.id ? c.devT<uint32_t>("wf.id", n + 1) : nullptr;
+            if (n) {
+                if (!v.pos || !v.len) fail(FGSS_ERR_INVALID, "null record arrays");
+                FGSS_CK(cudaMemcpyAsync(pos, v.pos, n * 4, cudaMemcpyHostToDevice, c.stream));
+                FGSS_CK(cudaMemcpyAsync(ln, v.len, n * 4, cudaMemcpyHostToDevice, c.stream));
+                if (id) FGSS_CK(cudaMemcpyAsync(id, v.id, n * 4, cudaMemcpyHostToDevice, c.stream));
+                memcpy(len.data(), v.len, n * 4);
+            }
+            if (v.n_tokens) {
+                if (!v.tokens) fail(FGSS_ERR_INVALID, "null token array");
+                FGSS_CK(cudaMemcpyAsync(tok, v.tokens, v.n_tokens * 4, cudaMemcpyHostToDevice, c.stream));
+            }
+            v.pos = pos;
+            v.len = ln;
+            v.tokens = tok;
+            v.id = id;
+            v.on_device = 1;
+        } else if (n) {
+            FGSS_CK(cudaMemcpyAsync(len.data(), v.len, n * 4, cudaMemcpyDeviceToHost, c.stream));
+        }
+        c.sync();
+        // contiguous query ranges of about equal work (candidates grow with size^2)
+        std::vector<uint64_t> cut{0};
+        {
+            double tot = 0;
+            for (uint64_t i = 0; i < n; i++) tot += (double)len[i] * len[i] + 1.0;
+            double acc = 0;
+            uint64_t i = 0;
+            for (int k = 1; k < n_shards; k++) {
+                const double target = tot * k / n_shards;
+                while (i < n && acc + (double)len[i] * len[i] + 1.0 <= target) acc += (double)len[i] * len[i] + 1.0, i++;
+                cut.push_back(std::max(cut.back(), i));
+            }
+            cut.push_back(n);
+        }
+        FILE* f = fopen(path, format == FGSS_OUT_BINARY ? "wb" : "w");
+        if (!f) fail(FGSS_ERR_IO, std::string("cannot open ") + path);
+        // writer thread: formats and writes one shard while the GPU joins the next;
+        // at most two shards wait in host memory
+        std::mutex mu;
+        std::condition_variable cv;
+        std::deque<fgss_pairs> queue;
+        bool closed = false, werr = false;
+        std::thread writer([&] {
+            std::vector<char> buf(1 << 20);
+            size_t used = 0;
+            auto flush = [&] {
+                if (used && fwrite(buf.data(), 1, used, f) != used) werr = true;
+                used = 0;
+            };
+            for (;;) {
+                fgss_pairs p;
+                {
+                    std::unique_lock<std::mutex> lk(mu);
+                    cv.wait(lk, [&] { return closed || !queue.empty(); });
+                    if (queue.empty()) break;
+                    p = queue.front();
+                    queue.pop_front();
+                }
+                cv.notify_all();
+                for (uint64_t i = 0; i < p.n; i++) {
+                    if (used + 64 > buf.size()) flush();
+                    if (format == FGSS_OUT_TEXT) {
+                        // the reference's line (block.cu:193)
+                        used += (size_t)snprintf(buf.data() + used, 64, "%d %d %f\n", (int)p.id_q[i], (int)p.id_s[i],
+                                                 (double)p.sim[i]);
+                    } else {
+                        memcpy(buf.data() + used, &p.id_q[i], 4);
+                        memcpy(buf.data() + used + 4, &p.id_s[i], 4);
+                        memcpy(buf.data() + used + 8, &p.sim[i], 4);
+                        used += 12;
+                    }
+                }
+                fgss_pairs_free(&p);
+            }
+            flush();
+        });
+        auto finish = [&] {
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                closed = true;
+            }
+            cv.notify_all();
+            writer.join();
+            for (auto& p : queue) fgss_pairs_free(&p);
+            queue.clear();
+        };
+        fgss_stats total;
+        memset(&total, 0, sizeof total);
+        try {
+            for (int k = 0; k < n_shards; k++) {
+                if (cut[k + 1] == cut[k]) continue;
+                fgss_join_opts o = *opts;
+                o.query_begin = cut[k];
+                o.query_end = cut[k + 1];
+                o.no_graph = 1;  // shards differ only in their query range: one set of buffers
+                fgss_pairs p;
+                fgss_stats st;
+                run_joins(c, &v, &o, 1, &p, &st);
+                total.candidates += st.candidates;
+                total.intersections += st.intersections;
+                total.results += st.results;
+                total.index_entries = st.index_entries;
+                total.probe_tokens += st.probe_tokens;
+                total.window_entries += st.window_entries;
+                total.verified += st.verified;
+                total.heavy_queries += st.heavy_queries;
+                total.overflow_retries += st.overflow_retries;
+                total.ms_total += st.ms_total;
+                total.ms_index += st.ms_index;
+                total.ms_filter += st.ms_filter;
+                total.ms_verify += st.ms_verify;
+                total.ms_output += st.ms_output;
+                total.ms_probe += st.ms_probe;
+                total.merged_tokens += st.merged_tokens;
+                total.launches += st.launches;
+                total.predicted_candidates += st.predicted_candidates;
+                total.predicted_results += st.predicted_results;
+                std::unique_lock<std::mutex> lk(mu);
+                cv.wait(lk, [&] { return queue.size() < 2; });
+                queue.push_back(p);
+                lk.unlock();
+                cv.notify_all();
+            }
+        } catch (...) {
+            finish();
+            fclose(f);
+            throw;
+        }
+        finish();
+        if (fclose(f) != 0) werr = true;
+        if (werr) fail(FGSS_ERR_IO, std::string("write failed: ") + path);
+        if (stats) *stats = total;
+    });
 }
 
 fgss_status fgss_autotune(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_join_opts* opts, int reps,

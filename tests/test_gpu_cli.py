@@ -57,3 +57,15 @@ def test_rs_form_matches_oracle(tmp_path):
                        "--pad", "--distinct", "--method", "batched"])
     assert len(want) > 0 and lines == want
     assert cnt["Results"] == st["results"] and cnt["Candidates"] == st["candidates"]
+
+
+def test_streamed_output_file(tmp_path):
+    text = datagen.titles(3000, seed=23)
+    f = tmp_path / "titles.txt"
+    f.write_bytes(text)
+    lines, cnt = _run(["-f", str(f), "-q", "3", "-t", "0.7", "--pad", "--distinct"])
+    out = tmp_path / "pairs.txt"
+    none, cnt2 = _run(["-f", str(f), "-q", "3", "-t", "0.7", "--pad", "--distinct", "--out", str(out),
+                       "--shards", "3", "--method", "batched"])
+    assert none == [] and len(lines) > 0
+    assert out.read_text().splitlines() == lines and cnt2 == cnt

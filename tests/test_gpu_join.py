@@ -358,3 +358,19 @@ def test_graph_captured_after_first_call_overflowed(ctx):
         for got, (ref, st) in zip(outs, refs):
             _check_same(got, ref, st)
             assert got.stats["overflow_retries"] == 0
+
+
+@pytest.mark.parametrize("shards", [1, 5])
+def test_streamed_output_equals_the_pairs(ctx, titles_sets, tmp_path, shards):
+    """fgss_selfjoin_to_file: the text file equals the printed pairs line for line,
+    the binary file holds the same (id, id, sim) records, the counters add up."""
+    s = titles_sets
+    ref = ctx.selfjoin(s, 0.7, method="batched")
+    st = ctx.selfjoin_to_file(s, 0.7, str(tmp_path / "p.txt"), fmt="text", shards=shards)
+    assert (tmp_path / "p.txt").read_text().splitlines() == ref.lines()
+    for k in ("candidates", "intersections", "results"):
+        assert st[k] == ref.stats[k]
+    ctx.selfjoin_to_file(s, 0.7, str(tmp_path / "p.bin"), fmt="binary", shards=shards, method="plain")
+    rec = np.fromfile(tmp_path / "p.bin", dtype=np.dtype([("q", "<u4"), ("s", "<u4"), ("sim", "<f4")]))
+    assert np.array_equal(rec["q"], ref.id_q) and np.array_equal(rec["s"], ref.id_s)
+    assert np.array_equal(rec["sim"], ref.sim)
