@@ -339,7 +339,7 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
             export_pairs(c, *js[i], opts[i], &outs[i]);
         }
         report_stats(c, v, stats, launch_counter() - launches0, n);
-        if (g && plan.valid && g->failed_captures < kMaxCaptureTries) {
+        if (g && g->failed_captures < kMaxCaptureTries) {
             // capture the same batch (index build included) for later calls
             plan.capture = true;
             const unsigned long long l0 = launch_counter();

@@ -4,20 +4,21 @@
 // filtering.cu:76-141, checking.cu:93-175, block.cu:184-197), organised for
 // throughput:
 //   * k_windows: one warp per query computes the id window [q+1, send) of
-//     every probe token's list by binary search, for all queries at once
-//     (massively parallel, latency hidden by occupancy), and the per-query
-//     window total that sizes work items.
-//   * k_fused: persistent CTAs pull work items (runs of queries of one join).
-//     Per query: the query's tokens and term bitmap go to shared memory, the
-//     precomputed windows are read with one coalesced load, window entries are
-//     accumulated into a shared-memory slot table (64-bit CAS per entry) that
-//     also appends every newly occupied slot to a list, and a lane-persistent
-//     loop drains that list: each lane takes the next slot, decides whether it
-//     is a reference candidate and whether a merge can still reach floor(min
-//     overlap), then merges the source's tokens 16 bytes per step against the
-//     query bitmap, taking the next slot as soon as it is done.  Lanes stay
-//     converged on the same short loop body instead of diverging over
-//     candidates of different lengths.
+//     every probe token's list by binary search, for all queries at once, the
+//     prefix of the window sizes and the per-query total that sizes work items.
+//   * k_chunks: queries whose windows hold more entries than half the slot
+//     table get precomputed id-range chunk boundaries.
+//   * k_fused: persistent CTAs pull work items (runs of queries of one join,
+//     longest first, claimed one item ahead).  Per query: the query's tokens
+//     and a membership structure (bitmap, hashed set or hashed bitmap) go to
+//     shared memory; per chunk the window entries are accumulated into a
+//     shared-memory slot table (64-bit CAS per entry) that also appends every
+//     newly occupied slot to a list, and a lane-persistent loop drains that
+//     list: each lane takes the next slot, decides whether it is a reference
+//     candidate and whether a merge can still reach floor(min overlap), then
+//     merges the source's tokens 8 per step against the membership structure,
+//     taking the next slot as soon as it is done; when at most a few merges
+//     remain the warp takes them together, 32 tokens per step.
 #pragma once
 
 #include "join_kernels.cuh"

@@ -90,7 +90,6 @@ void join_output(Ctx& c, JoinState& J, uint64_t* keys, uint32_t* vals, const uin
 // same batch is captured into a CUDA graph (batch.cu).
 struct BatchPlan {
     bool capture = false;             // issue device work only, with these decisions
-    bool valid = true;                // false: do not capture this run
     TuneEntry te;
     std::vector<uint32_t> K;          // work items per join
     uint64_t nitems = 0;
