@@ -76,15 +76,18 @@ __global__ void k_items(const uint64_t* __restrict__ pre, uint32_t n, const uint
 }
 
 // Item sort keys: ~cost (so ascending order = descending cost), value = item index.
+// Sort key of a work item: its cost as a float's exponent and top 7 mantissa
+// bits (the longest-first order needs no more), complemented so an ascending
+// sort puts the costliest first; 16 bits, two radix passes.
 __global__ void k_item_keys(const uint64_t* __restrict__ pre, uint32_t n, const uint64_t* __restrict__ d_total,
-                            const uint4* __restrict__ items, uint32_t K, uint32_t base, uint64_t* __restrict__ key,
+                            const uint4* __restrict__ items, uint32_t K, uint32_t base, uint32_t* __restrict__ key,
                             uint32_t* __restrict__ val) {
     const uint64_t total = *d_total;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
         const uint4 it = items[k];
         const uint64_t b = it.y < n ? pre[it.y] : total;
         const uint64_t e = it.z < n ? pre[it.z] : total;
-        key[base + k] = ~(e - b);
+        key[base + k] = (~__float_as_uint((float)(e - b)) >> 16) & 0xffffu;
         val[base + k] = base + k;
     }
 }
@@ -316,7 +319,7 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
     }
     if (nitems > 1) {
         // longest-processing-time order: sort items by descending cost
-        uint64_t* ikey = c.devT<uint64_t>(c.bpfx + "b.ikey", nitems + 1);
+        uint32_t* ikey = c.devT<uint32_t>(c.bpfx + "b.ikey", nitems + 1);
         uint32_t* ival = c.devT<uint32_t>(c.bpfx + "b.ival", nitems + 1);
         uint4* sorted = c.devT<uint4>(c.bpfx + "b.items2", nitems + 1);
         uint64_t off2 = 0;
@@ -327,7 +330,7 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
             FGSS_LAUNCH_CK();
             off2 += K[i];
         }
-        radix_sort<uint64_t, uint32_t>(c, ikey, ival, nitems, nullptr, 0, 64, (c.bpfx + "b.isort").c_str());
+        radix_sort<uint32_t, uint32_t>(c, ikey, ival, nitems, nullptr, 0, 16, (c.bpfx + "b.isort").c_str());
         k_permute_items<<<grid_for(nitems, 128), 128, 0, c.stream>>>(items, ival, nitems, sorted);
         FGSS_LAUNCH_CK();
         items = sorted;
