@@ -161,6 +161,53 @@ static __global__ void k_chunks(JoinArgs a, const uint32_t* __restrict__ poff, c
     }
 }
 
+// Bitmap filter (the bitwise overlap bound of Sandes, Teodoro and Melo for
+// exact set similarity joins): every record's tokens hashed into 256 bits.  A
+// bit set in only one of two bitmaps comes from at least one token in only one
+// of the two records, so |x & y| <= (|x| + |y| - popcount(b(x) ^ b(y))) / 2.
+// Warp per record (a long record's bitmap is nearly full and bounds little,
+// but it is exact, so the bound holds for every pair).
+
+__device__ __forceinline__ uint32_t bmap_bit(uint32_t x) { return (x * 0x9E3779B1u) >> 24; }
+
+static __global__ void k_bitmaps(JoinArgs a, uint4* __restrict__ bmap) {
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t lane = lane_id();
+    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < a.n; r += warps) {
+        const uint32_t l = a.len[r];
+        const uint32_t* t = a.tok + a.pos[r];
+        uint32_t w0 = 0, w1 = 0, w2 = 0, w3 = 0, w4 = 0, w5 = 0, w6 = 0, w7 = 0;
+        for (uint32_t j = lane; j < l; j += 32) {
+            const uint32_t b = bmap_bit(__ldg(t + j));
+            const uint32_t m = 1u << (b & 31), wi = b >> 5;
+            w0 |= wi == 0 ? m : 0u;
+            w1 |= wi == 1 ? m : 0u;
+            w2 |= wi == 2 ? m : 0u;
+            w3 |= wi == 3 ? m : 0u;
+            w4 |= wi == 4 ? m : 0u;
+            w5 |= wi == 5 ? m : 0u;
+            w6 |= wi == 6 ? m : 0u;
+            w7 |= wi == 7 ? m : 0u;
+        }
+        w0 = __reduce_or_sync(kFull, w0);
+        w1 = __reduce_or_sync(kFull, w1);
+        w2 = __reduce_or_sync(kFull, w2);
+        w3 = __reduce_or_sync(kFull, w3);
+        w4 = __reduce_or_sync(kFull, w4);
+        w5 = __reduce_or_sync(kFull, w5);
+        w6 = __reduce_or_sync(kFull, w6);
+        w7 = __reduce_or_sync(kFull, w7);
+        if (lane == 0) {
+            bmap[2 * r] = make_uint4(w0, w1, w2, w3);
+            bmap[2 * r + 1] = make_uint4(w4, w5, w6, w7);
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t popc_xor(uint4 a, uint4 b) {
+    return __popc(a.x ^ b.x) + __popc(a.y ^ b.y) + __popc(a.z ^ b.z) + __popc(a.w ^ b.w);
+}
+
 struct FusedArgs {
     const uint32_t* poff;    // per query: first probe window
     const uint2* win;
@@ -169,6 +216,7 @@ struct FusedArgs {
     const uint32_t* wpre;    // per probe window: entries of the query's earlier windows
     const uint2* qchunk;     // per query: (first boundary in cbuf, number of chunks)
     const uint32_t* cbuf;    // chunk boundaries: per inner boundary, first entry of each probe window
+    const uint4* bmap;       // per record: 256-bit token bitmap (two uint4)
 };
 
 // Query-token membership, three forms chosen per query (the same for every
@@ -278,6 +326,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     uint32_t* qtok = reinterpret_cast<uint32_t*>(smem + Lay::off_qtok);
     uint32_t* bm = reinterpret_cast<uint32_t*>(smem + Lay::off_bm);
     __shared__ uint32_t s_L, s_sp, s_nocc, s_next, s_cand, s_win;
+    __shared__ uint4 s_qbm[2];  // the query's bitmap
     __shared__ uint32_t s_sa[48], s_sb[48], s_sc[48];
     __shared__ uint32_t wsum[33];
 
@@ -313,6 +362,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
         if (staged) qtok[j] = x;
         bm_insert(bm, qmode, x);
     }
+    if (tid < 2) s_qbm[tid] = fa.bmap[2 * q + tid];
     // one chunk that fits the slot table (the common case): the pre-pass's
     // window prefix is used as is, with no block-wide scan
     const bool one_chunk = nch == 1 && qm.w <= Lay::cap;
@@ -535,8 +585,15 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                             // resume right after the last match (or at c when its position was not kept)
                             k = smx != kSmaxUnknown ? smx + 1 : c;
                             p0 = k;
-                            if (k >= ls || cnt + min(ls - k, qrest) < im) tally(c, k);
-                            else have = true;
+                            if (k >= ls || cnt + min(ls - k, qrest) < im) {
+                                tally(c, k);
+                            } else {
+                                // bitmap bound on the whole overlap: below floor(min overlap), no merge
+                                const uint4* sb = fa.bmap + 2 * s;
+                                const uint32_t pc = popc_xor(s_qbm[0], __ldg(sb)) + popc_xor(s_qbm[1], __ldg(sb + 1));
+                                if (lq + ls < 2 * im + pc) tally(c, k);
+                                else have = true;
+                            }
                         }
                     }
                 }
