@@ -8,6 +8,7 @@
 //     prefix of the window sizes and the per-query total that sizes work items.
 //   * k_chunks: queries whose windows hold more entries than half the slot
 //     table get precomputed id-range chunk boundaries.
+//   * k_bitmaps: a 256-bit token bitmap per record (the bitmap filter).
 //   * k_fused: persistent CTAs pull work items (runs of queries of one join,
 //     longest first, claimed one item ahead).  Per query: the query's tokens
 //     and a membership structure (bitmap, hashed set or hashed bitmap) go to
@@ -15,7 +16,8 @@
 //     shared-memory slot table (64-bit CAS per entry) that also appends every
 //     newly occupied slot to a list, and a lane-persistent loop drains that
 //     list: each lane takes the next slot, decides whether it is a reference
-//     candidate and whether a merge can still reach floor(min overlap), then
+//     candidate and whether a merge can still reach floor(min overlap) (by
+//     positions, then by a 256-bit bitmap bound), then
 //     merges the source's tokens 8 per step against the membership structure,
 //     taking the next slot as soon as it is done; when at most a few merges
 //     remain the warp takes them together, 32 tokens per step.
