@@ -244,7 +244,10 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         uint32_t* pred = c.devT<uint32_t>(J.pfx("pred"), n + 1);
         pre[i] = c.devT<uint64_t>(J.pfx("cpre"), n + 1);
         uint4* meta = c.devT<uint4>(J.pfx("meta"), n + 1);
-        uint4* bmap = c.devT<uint4>(J.pfx("bmap"), 2 * n + 2);
+        // bitmap filter width: 512 bits when records average more than 96 tokens
+        // (a 256-bit bitmap of a long record is too full to bound much)
+        const uint32_t bmw = J.in.n_tokens > 96ull * std::max<uint64_t>(n, 1) ? 4u : 2u;
+        uint4* bmap = c.devT<uint4>(J.pfx("bmap"), (uint64_t)bmw * n + 4);
         uint2* qchunk = c.devT<uint2>(J.pfx("qchunk"), n + 1);
         const uint64_t cbuf_cap = 2 * J.in.n_tokens + (1u << 20);  // overflowing queries bisect instead
         uint32_t* cbuf = c.devT<uint32_t>(J.pfx("cbuf"), cbuf_cap);
@@ -256,6 +259,7 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         hf[i].qchunk = qchunk;
         hf[i].cbuf = cbuf;
         hf[i].bmap = bmap;
+        hf[i].bmw = bmw;
         if (n == 0) continue;
         // windows of every probe token (exact per-query work), chunk splits, then
         // features and the learned estimate, then the work-item cost prefix
@@ -264,7 +268,7 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         FGSS_CK(cudaMemsetAsync(cused, 0, 8, c.stream));
         k_windows<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wpre, wtot, meta);
         FGSS_LAUNCH_CK();
-        k_bitmaps<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, bmap);
+        k_bitmaps<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, bmap, bmw);
         FGSS_LAUNCH_CK();
         k_chunks<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wtot, cap_entries,
                                                                             qchunk, cbuf, cbuf_cap, cused);

@@ -8,7 +8,7 @@
 //     prefix of the window sizes and the per-query total that sizes work items.
 //   * k_chunks: queries whose windows hold more entries than half the slot
 //     table get precomputed id-range chunk boundaries.
-//   * k_bitmaps: a 256-bit token bitmap per record (the bitmap filter).
+//   * k_bitmaps: a token bitmap per record (the bitmap filter).
 //   * k_fused: persistent CTAs pull work items (runs of queries of one join,
 //     longest first, claimed one item ahead).  Per query: the query's tokens
 //     and a membership structure (bitmap, hashed set or hashed bitmap) go to
@@ -17,7 +17,7 @@
 //     newly occupied slot to a list, and a lane-persistent loop drains that
 //     list: each lane takes the next slot, decides whether it is a reference
 //     candidate and whether a merge can still reach floor(min overlap) (by
-//     positions, then by a 256-bit bitmap bound), then
+//     positions, then by a 256- or 512-bit bitmap bound), then
 //     merges the source's tokens 8 per step against the membership structure,
 //     taking the next slot as soon as it is done; when at most a few merges
 //     remain the warp takes them together, 32 tokens per step.
@@ -164,45 +164,31 @@ static __global__ void k_chunks(JoinArgs a, const uint32_t* __restrict__ poff, c
 }
 
 // Bitmap filter (the bitwise overlap bound of Sandes, Teodoro and Melo for
-// exact set similarity joins): every record's tokens hashed into 256 bits.  A
+// exact set similarity joins): every record's tokens hashed into a bitmap.  A
 // bit set in only one of two bitmaps comes from at least one token in only one
 // of the two records, so |x & y| <= (|x| + |y| - popcount(b(x) ^ b(y))) / 2.
 // Warp per record (a long record's bitmap is nearly full and bounds little,
-// but it is exact, so the bound holds for every pair).
-
-__device__ __forceinline__ uint32_t bmap_bit(uint32_t x) { return (x * 0x9E3779B1u) >> 24; }
-
-static __global__ void k_bitmaps(JoinArgs a, uint4* __restrict__ bmap) {
+// but it is exact, so the bound holds for every pair).  Width: bmw uint4 per
+// record, 2 (256 bits) or 4 (512 bits, for joins of longer records).
+static __global__ void k_bitmaps(JoinArgs a, uint4* __restrict__ bmap, uint32_t bmw) {
+    __shared__ uint32_t sw[8][16];  // launched with 256 threads: a bitmap per warp
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t lane = lane_id();
+    const uint32_t lane = lane_id(), wl = threadIdx.x >> 5;
+    const uint32_t shift = bmw == 4 ? 23 : 24;  // bit index: top 9 or 8 bits of a multiplicative hash
     for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < a.n; r += warps) {
+        if (lane < 16) sw[wl][lane] = 0;
+        __syncwarp();
         const uint32_t l = a.len[r];
         const uint32_t* t = a.tok + a.pos[r];
-        uint32_t w0 = 0, w1 = 0, w2 = 0, w3 = 0, w4 = 0, w5 = 0, w6 = 0, w7 = 0;
         for (uint32_t j = lane; j < l; j += 32) {
-            const uint32_t b = bmap_bit(__ldg(t + j));
-            const uint32_t m = 1u << (b & 31), wi = b >> 5;
-            w0 |= wi == 0 ? m : 0u;
-            w1 |= wi == 1 ? m : 0u;
-            w2 |= wi == 2 ? m : 0u;
-            w3 |= wi == 3 ? m : 0u;
-            w4 |= wi == 4 ? m : 0u;
-            w5 |= wi == 5 ? m : 0u;
-            w6 |= wi == 6 ? m : 0u;
-            w7 |= wi == 7 ? m : 0u;
+            const uint32_t b = (__ldg(t + j) * 0x9E3779B1u) >> shift;
+            atomicOr(&sw[wl][b >> 5], 1u << (b & 31));
         }
-        w0 = __reduce_or_sync(kFull, w0);
-        w1 = __reduce_or_sync(kFull, w1);
-        w2 = __reduce_or_sync(kFull, w2);
-        w3 = __reduce_or_sync(kFull, w3);
-        w4 = __reduce_or_sync(kFull, w4);
-        w5 = __reduce_or_sync(kFull, w5);
-        w6 = __reduce_or_sync(kFull, w6);
-        w7 = __reduce_or_sync(kFull, w7);
-        if (lane == 0) {
-            bmap[2 * r] = make_uint4(w0, w1, w2, w3);
-            bmap[2 * r + 1] = make_uint4(w4, w5, w6, w7);
-        }
+        __syncwarp();
+        if (lane < bmw)
+            bmap[bmw * r + lane] =
+                make_uint4(sw[wl][4 * lane], sw[wl][4 * lane + 1], sw[wl][4 * lane + 2], sw[wl][4 * lane + 3]);
+        __syncwarp();
     }
 }
 
@@ -218,7 +204,8 @@ struct FusedArgs {
     const uint32_t* wpre;    // per probe window: entries of the query's earlier windows
     const uint2* qchunk;     // per query: (first boundary in cbuf, number of chunks)
     const uint32_t* cbuf;    // chunk boundaries: per inner boundary, first entry of each probe window
-    const uint4* bmap;       // per record: 256-bit token bitmap (two uint4)
+    const uint4* bmap;       // per record: token bitmap of bmw uint4
+    uint32_t bmw;            // 2 (256 bits) or 4 (512 bits)
 };
 
 // Query-token membership, three forms chosen per query (the same for every
@@ -328,7 +315,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     uint32_t* qtok = reinterpret_cast<uint32_t*>(smem + Lay::off_qtok);
     uint32_t* bm = reinterpret_cast<uint32_t*>(smem + Lay::off_bm);
     __shared__ uint32_t s_L, s_sp, s_nocc, s_next, s_cand, s_win;
-    __shared__ uint4 s_qbm[2];  // the query's bitmap
+    __shared__ uint4 s_qbm[4];  // the query's bitmap
     __shared__ uint32_t s_sa[48], s_sb[48], s_sc[48];
     __shared__ uint32_t wsum[33];
 
@@ -364,7 +351,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
         if (staged) qtok[j] = x;
         bm_insert(bm, qmode, x);
     }
-    if (tid < 2) s_qbm[tid] = fa.bmap[2 * q + tid];
+    if (tid < fa.bmw) s_qbm[tid] = fa.bmap[fa.bmw * q + tid];
     // one chunk that fits the slot table (the common case): the pre-pass's
     // window prefix is used as is, with no block-wide scan
     const bool one_chunk = nch == 1 && qm.w <= Lay::cap;
@@ -591,8 +578,9 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                                 tally(c, k);
                             } else {
                                 // bitmap bound on the whole overlap: below floor(min overlap), no merge
-                                const uint4* sb = fa.bmap + 2 * s;
-                                const uint32_t pc = popc_xor(s_qbm[0], __ldg(sb)) + popc_xor(s_qbm[1], __ldg(sb + 1));
+                                const uint4* sb = fa.bmap + fa.bmw * s;
+                                uint32_t pc = popc_xor(s_qbm[0], __ldg(sb)) + popc_xor(s_qbm[1], __ldg(sb + 1));
+                                if (fa.bmw == 4) pc += popc_xor(s_qbm[2], __ldg(sb + 2)) + popc_xor(s_qbm[3], __ldg(sb + 3));
                                 if (lq + ls < 2 * im + pc) tally(c, k);
                                 else have = true;
                             }
