@@ -111,7 +111,8 @@ class Clocks:
 
     def __init__(self, index):
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % os.getpid())
+        import tempfile
+        self.path = os.path.join(tempfile.gettempdir(), "fgss_bench_clocks_%d.csv" % os.getpid())
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
