@@ -183,7 +183,7 @@ typedef struct fgss_stats {
     uint64_t merged_tokens;   /* source tokens the fused kernel's merges read */
     uint64_t launches;        /* kernels launched by the call */
     uint64_t predicted_candidates; /* batched method with use_model: the learned model's estimates */
-    uint64_t predicted_results;    /* of candidates and results (0 otherwise; the exact counts judge them) */
+    uint64_t predicted_results;    /* of candidates and results (0 otherwise; compare with the exact counts) */
 } fgss_stats;
 
 typedef struct fgss_pairs {
