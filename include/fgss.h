@@ -316,8 +316,10 @@ fgss_status fgss_dev_exclusive_scan_u32(fgss_ctx* ctx, const uint32_t* in, uint3
  *   - Scratch is a fixed 256 KiB array in the library (one per device, kept
  *     until the process exits), so n is limited to 268,435,456 elements;
  *     larger n returns FGSS_ERR_CAPACITY (message in fgss_last_error(NULL)).
- *   - The first call on a device looks the array's device address up once
- *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - Calls look the array's device address up (cudaGetSymbolAddress)
+ *     whenever their stream is not capturing, so a device reset never leaves
+ *     a stale address behind; make the first call on a device, and the first
+ *     after a device reset, before any stream capture.
  *   - Every call shares that one array: calls that overlap on the GPU (other
  *     streams, other host threads) race and must be serialized by the caller.
  * Same result as fgss_dev_exclusive_scan_u32 (out may alias in). */

@@ -8,7 +8,7 @@
 //                                                          tokenized on the GPU
 // Options of the second form: --pad (pad q-grams), --distinct (one token per
 // distinct gram instead of gram + occurrence), --kmer (canonical k-mers, k = q),
-// --method plain|batched, --bounds reference|exact, --write-bin <path> (also
+// --method batched|plain (default batched), --bounds reference|exact, --write-bin <path> (also
 // write the tokenized .bin and .bin.loc), --device <n>, -s <text>: an R-S
 // join of the -f file (R) with this one (S) over one vocabulary, printing
 // "id_in_R id_in_S similarity" (no reference counterpart), and
@@ -68,7 +68,7 @@ int main(int argc, char** argv) {
     std::string bin_path, text_path, second_path, write_bin, out_path;
     int shards = 4, out_binary = 0;
     float threshold = 0.f;
-    int q = 3, pad = 0, suffix = 1, kmer = 0, method = FGSS_METHOD_PLAIN, bounds = FGSS_BOUNDS_REFERENCE;
+    int q = 3, pad = 0, suffix = 1, kmer = 0, method = FGSS_METHOD_BATCHED, bounds = FGSS_BOUNDS_REFERENCE;
     int device = 0;
     char verbose = 0, debug = 0;
     if (argv[1][0] == '-') {

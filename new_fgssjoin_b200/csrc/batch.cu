@@ -493,14 +493,3 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
 }
 
 }  // namespace fgss
-
-#ifdef FGSS_PHASE_PROFILE
-// Reads and clears the fused kernel's per-phase cycle counters (profiling builds only).
-extern "C" int fgss_phase_cycles(unsigned long long* out, int n) {
-    if (n > 8) n = 8;
-    if (cudaMemcpyFromSymbol(out, fgss::g_phase_cycles, n * sizeof(unsigned long long)) != cudaSuccess) return -1;
-    unsigned long long z[8] = {};
-    cudaMemcpyToSymbol(fgss::g_phase_cycles, z, sizeof z);
-    return n;
-}
-#endif

@@ -27,24 +27,6 @@
 
 namespace fgss {
 
-// Optional per-phase cycle accounting of the fused kernel (thread 0 of every
-// CTA), compiled in only with -DFGSS_PHASE_PROFILE; no effect otherwise.
-#ifdef FGSS_PHASE_PROFILE
-__device__ unsigned long long g_phase_cycles[8];
-#define FGSS_PHASE_START() long long fgss_pt_ = clock64()
-#define FGSS_PHASE(i)                                                                   \
-    do {                                                                                \
-        if (threadIdx.x == 0) {                                                         \
-            long long n_ = clock64();                                                   \
-            atomicAdd(&g_phase_cycles[i], (unsigned long long)(n_ - fgss_pt_));         \
-            fgss_pt_ = n_;                                                              \
-        }                                                                               \
-    } while (0)
-#else
-#define FGSS_PHASE_START() (void)0
-#define FGSS_PHASE(i) (void)0
-#endif
-
 // Slot word: source id (32) | query position of the last match (11) |
 // source position of the last match (11; 2047 = too large to keep) |
 // number of prefix matches (10).
@@ -338,7 +320,6 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     const uint32_t qmode = a.n_terms <= Lay::BW * 32 ? QM_EXACT : (lq <= kQHashMax ? QM_HASH : QM_BLOOM);
     const uint8_t* sidep = SIDED ? a.side : nullptr;  // R-S join: skip sources on the query's own side
     const uint8_t side_q = SIDED ? __ldg(sidep + q) : 0;
-    FGSS_PHASE_START();
     const uint32_t* qt = a.tok + qm.x;
     const bool staged = lq <= Lay::QC;
     const uint32_t* qsrc = staged ? qtok : qt;  // query tokens: shared memory, or HBM for long records
@@ -382,7 +363,6 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
         }
         for (;;) {
             __syncthreads();
-            FGSS_PHASE(0);  // staging / previous chunk's clear
             const uint32_t sp = s_sp;
             if (sp == 0) break;
             const uint32_t ra = s_sa[sp - 1], rb = s_sb[sp - 1], tag = s_sc[sp - 1];
@@ -433,7 +413,6 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                 }
             }
             __syncthreads();
-            FGSS_PHASE(1);  // chunk windows + scan
             const uint32_t L = s_L;
             if (L > Lay::cap && rb - ra > 1) {
                 if (tid == 0) {  // bisect an oversized range; the lower half first
@@ -511,7 +490,6 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                 }
             }
             __syncthreads();
-            FGSS_PHASE(2);  // accumulate
             // lane-persistent decide + merge over the occupied slots; the whole warp
             // iterates until every lane has drained the list, and lanes without a
             // candidate take the next slots with one atomic per warp
@@ -634,7 +612,6 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
             my_cand = warp_sum(my_cand);
             if (lane == 0 && my_cand) atomicAdd(&s_cand, my_cand);
             __syncthreads();
-            FGSS_PHASE(3);  // decide + merge
             for (uint32_t i2 = tid; i2 < nocc; i2 += NT) slots[occ[i2]] = kEmptySlot;
         }
     }

@@ -29,16 +29,24 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 uint32_t* g_scratch_addr[kMaxDevices] = {};
 
-// Device address of g_scan_scratch on the current device (looked up once per
-// device; the host-side name of the array is not a device address).
-uint32_t* scratch_for_current_device(int* err_dev) {
+// Device address of g_scan_scratch on the current device (the host-side name
+// of the array is not a device address).  It is looked up again on every call
+// whose stream is not capturing, so a device reset (or the primary context
+// being torn down and re-created), which moves the array, never leaves a stale
+// address behind; a call under stream capture takes the address of the last
+// uncaptured call on this device.
+uint32_t* scratch_for_current_device(cudaStream_t stream, int* err_dev) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         *err_dev = dev;
         return nullptr;
     }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    bool capturing = true;  // if the stream cannot tell, keep out of the lookup
+    if (cudaStreamIsCapturing(stream, &cs) == cudaSuccess) capturing = cs != cudaStreamCaptureStatusNone;
+    else (void)cudaGetLastError();
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
+    if (!capturing) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_scan_scratch) != cudaSuccess) {
             (void)cudaGetLastError();
@@ -47,6 +55,7 @@ uint32_t* scratch_for_current_device(int* err_dev) {
         }
         g_scratch_addr[dev] = static_cast<uint32_t*>(p);
     }
+    if (!g_scratch_addr[dev]) *err_dev = dev;
     return g_scratch_addr[dev];
 }
 
@@ -68,12 +77,13 @@ extern "C" fgss_status fgss_dev_exclusive_scan_u32_noalloc(const uint32_t* in, u
         return FGSS_ERR_CAPACITY;
     }
     int dev = -1;
-    uint32_t* sums = scratch_for_current_device(&dev);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    uint32_t* sums = scratch_for_current_device(s, &dev);
     if (!sums) {
-        set_thread_error("fgss_dev_exclusive_scan_u32_noalloc: no scratch address on device " + std::to_string(dev));
+        set_thread_error("fgss_dev_exclusive_scan_u32_noalloc: no scratch address on device " + std::to_string(dev) +
+                         " (the first call on a device, and the first after a device reset, must not be captured)");
         return FGSS_ERR_CUDA;
     }
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     // Every tile sum the later kernels read is written by k_scan_tiles first,
     // so the array's contents from an earlier call never leak into this one.
     k_scan_tiles<uint32_t><<<(unsigned)ntiles, kScanThreads, 0, s>>>(in, out, sums, n, nullptr);

@@ -18,8 +18,10 @@ constexpr int kScanThreads = 256;
 constexpr int kScanItems = 16;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
+// `in` may alias `out` (in-place scans): each element is read and written by
+// the same thread, the read before the block's barrier and the write after.
 template <typename T>
-__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const T* __restrict__ in, T* out, T* tile_sums,
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const T* in, T* out, T* tile_sums,
                                                               uint64_t n_cap, const uint64_t* d_n) {
     __shared__ T wsum[33];
     const uint64_t n = d_n ? min(*d_n, n_cap) : n_cap;

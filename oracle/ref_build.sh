@@ -4,7 +4,7 @@
 # tests run it to pin the tokenizer's token and term counts.  The reference's
 # join is CUDA and is not built or run here.
 set -e
-REF=${REF:-/root/reference}
+REF=${FGSS_REFERENCE:-/root/reference}  # where the reference checkout lies
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 [ -d "$REF/src" ] || { echo "reference sources not found at $REF; nothing to build"; exit 0; }

@@ -6,6 +6,8 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 GOLDEN = os.path.join(ROOT, "tests", "golden")
+# The reference checkout (CPU pins only; absent on GPU machines, where those tests skip).
+REFERENCE = os.environ.get("FGSS_REFERENCE", "/root/reference")
 
 
 def pytest_configure(config):

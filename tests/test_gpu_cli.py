@@ -39,7 +39,7 @@ def test_text_form_matches_oracle(tmp_path):
     mid, mpos, mlen, mtok = O.file_to_memory(ids, lens, tok)
     ref, st = O.join(mpos, mlen, mtok, nt, 0.8)
     want = ["%d %d %f" % (mid[q], mid[s], x) for q, s, x in zip(ref["q"], ref["s"], ref["sim"])]
-    for extra in ([], ["--method", "batched"]):
+    for extra in (["--method", "plain"], []):
         lines, cnt = _run(["-f", str(f), "-q", "3", "-t", "0.8", "--pad", "--distinct"] + extra)
         assert lines == want
         assert cnt == {"Candidates": st["candidates"], "Intersections": st["intersections"],

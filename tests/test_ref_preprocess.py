@@ -7,11 +7,11 @@ import subprocess
 
 import pytest
 
-from conftest import GOLDEN, ROOT
+from conftest import GOLDEN, REFERENCE, ROOT
 from oracle import oracle as O
 
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "preprocess")
-DBLP = "/root/reference/test/data/string/dblp_t_18k.txt"
+DBLP = os.path.join(REFERENCE, "test", "data", "string", "dblp_t_18k.txt")
 
 
 def _sdbm(b):

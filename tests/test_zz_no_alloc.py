@@ -23,6 +23,11 @@ def _noalloc(L, d_in, d_out, n, stream):
                                                  n, ctypes.c_void_p(stream))
 
 
+def _want(a):
+    incl = np.cumsum(a.astype(np.uint64))
+    return ((incl - a.astype(np.uint64)) & np.uint64(0xFFFFFFFF)).astype(np.uint32)  # wraps like uint32
+
+
 def test_noalloc_scan_matches_regular_scan_twice():
     L = F.load_library()
     torch.cuda.set_device(0)
@@ -40,9 +45,40 @@ def test_noalloc_scan_matches_regular_scan_twice():
             assert _noalloc(L, d_in, got, n, stream.cuda_stream) == 0
             torch.cuda.synchronize()
             assert torch.equal(got, ref)  # integer scan: exact
-            incl = np.cumsum(a.astype(np.uint64))
-            want = ((incl - a.astype(np.uint64)) & np.uint64(0xFFFFFFFF)).astype(np.uint32)  # wraps like uint32
-            assert np.array_equal(got.cpu().numpy().view(np.uint32), want)
+            assert np.array_equal(got.cpu().numpy().view(np.uint32), _want(a))
+
+
+def test_noalloc_scan_in_place():
+    """out == in: the header allows it, so check it against numpy."""
+    L = F.load_library()
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream(0)
+    rng = np.random.default_rng(7)
+    for n in (5_000_001, 4096):
+        a = rng.integers(0, 1 << 31, n).astype(np.uint32)
+        buf = torch.from_numpy(a.view(np.int32)).cuda()
+        assert _noalloc(L, buf, buf, n, stream.cuda_stream) == 0
+        torch.cuda.synchronize()
+        assert np.array_equal(buf.cpu().numpy().view(np.uint32), _want(a))
+
+
+def test_noalloc_scan_allocates_no_device_memory():
+    """After a first call, further calls leave the device's free memory as it was."""
+    L = F.load_library()
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream(0)
+    n = 3_000_000
+    a = np.arange(n, dtype=np.uint32) % 977
+    d_in = torch.from_numpy(a.view(np.int32)).cuda()
+    out = torch.empty_like(d_in)
+    assert _noalloc(L, d_in, out, n, stream.cuda_stream) == 0
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    for _ in range(3):
+        assert _noalloc(L, d_in, out, n, stream.cuda_stream) == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] == free0
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), _want(a))
 
 
 def test_noalloc_scan_rejects_sizes_beyond_its_scratch():
