@@ -295,6 +295,15 @@ fgss_status fgss_model_load(fgss_ctx* ctx, const char* path);
 fgss_status fgss_bounds_table(float threshold, int bounds, uint32_t max_len, uint16_t* probe, uint16_t* index,
                               uint32_t* min_size, uint32_t* max_size, uint32_t* need);
 
+/* Host-side overlap tables of one threshold (no device needed), per length sum
+ * S <= max_sum (<= 131070): cand_min[S], the smallest integer k that the
+ * positional test of src/fgssjoin/filtering.cu:130-132 does not reject
+ * (!(k < jac_min_overlap)); inter_min[S], checking.cu:110's
+ * floor(jac_min_overlap).  With fgss_bounds_table these are every bound the
+ * join reads.  Any output pointer may be NULL. */
+fgss_status fgss_overlap_table(float threshold, int bounds, uint32_t max_sum, uint32_t* cand_min,
+                               uint32_t* inter_min);
+
 /* ------------------------------------------------- device-level primitives */
 /* Stage kernels exposed for tests and callers that keep data on the device.
  * All pointers are device pointers; the work runs on the context's stream

@@ -21,8 +21,8 @@ prints and calls ``exit(1)``, src/util.cu:43-49).  There is no CPU fallback:
 every compute call goes through the CUDA library and fails loudly when it is
 missing or no B200 is present.
 """
-from .binding import (FgssError, Context, Sets, Pairs, ppjoin_format, lib_path, load_library, bounds_table,  # noqa: F401
+from .binding import (FgssError, Context, Sets, Pairs, ppjoin_format, lib_path, load_library, bounds_table, overlap_table,  # noqa: F401
                       METHOD_PLAIN, METHOD_BATCHED, BOUNDS_REFERENCE, BOUNDS_EXACT, EXPORTED_SYMBOLS)
 
-__all__ = ["FgssError", "Context", "Sets", "Pairs", "ppjoin_format", "lib_path", "load_library", "bounds_table",
+__all__ = ["FgssError", "Context", "Sets", "Pairs", "ppjoin_format", "lib_path", "load_library", "bounds_table", "overlap_table",
            "METHOD_PLAIN", "METHOD_BATCHED", "BOUNDS_REFERENCE", "BOUNDS_EXACT", "EXPORTED_SYMBOLS"]

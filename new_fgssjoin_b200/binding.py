@@ -19,7 +19,7 @@ EXPORTED_SYMBOLS = [
     "fgss_join_opts_default", "fgss_selfjoin", "fgss_selfjoin_batch", "fgss_rsjoin", "fgss_pairs_free",
     "fgss_pairs_print", "fgss_selfjoin_to_file",
     "fgss_model_train", "fgss_model_save", "fgss_model_load", "fgss_model_grad", "fgss_model_num_params",
-    "fgss_autotune", "fgss_bounds_table", "fgss_dev_exclusive_scan_u32", "fgss_dev_sort_pairs_u64",
+    "fgss_autotune", "fgss_bounds_table", "fgss_overlap_table", "fgss_dev_exclusive_scan_u32", "fgss_dev_sort_pairs_u64",
     "fgss_dev_exclusive_scan_u32_noalloc",
 ]
 
@@ -132,6 +132,7 @@ def load_library():
     L.fgss_autotune.argtypes = [ctypes.c_void_p, P(_View), P(_JoinOpts), ctypes.c_int, P(_TuneResult)]
     L.fgss_bounds_table.argtypes = [ctypes.c_float, ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.fgss_overlap_table.argtypes = [ctypes.c_float, ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
     _lib = L
     return L
 
@@ -151,6 +152,19 @@ def bounds_table(threshold, max_len, bounds="reference"):
     if st != 0:
         raise FgssError(st, "fgss_bounds_table failed")
     return probe, index, mins, maxs, need
+
+
+def overlap_table(threshold, max_sum, bounds="reference"):
+    """Host-side overlap tables (no GPU) per length sum: the smallest count the
+    positional filter keeps (cand_min) and floor(min overlap) (inter_min)."""
+    L = load_library()
+    mode = {"reference": BOUNDS_REFERENCE, "exact": BOUNDS_EXACT}.get(bounds, bounds)
+    cand = np.zeros(max_sum + 1, np.uint32)
+    inter = np.zeros(max_sum + 1, np.uint32)
+    st = L.fgss_overlap_table(ctypes.c_float(threshold), mode, max_sum, cand.ctypes.data, inter.ctypes.data)
+    if st != 0:
+        raise FgssError(st, "fgss_overlap_table failed")
+    return cand, inter
 
 
 def _check(L, ctx, st):

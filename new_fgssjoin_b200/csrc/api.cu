@@ -917,6 +917,19 @@ fgss_status fgss_bounds_table(float threshold, int bounds, uint32_t max_len, uin
     return FGSS_OK;
 }
 
+fgss_status fgss_overlap_table(float threshold, int bounds, uint32_t max_sum, uint32_t* cand_min,
+                               uint32_t* inter_min) {
+    if (max_sum > 2 * kMaxLen) return FGSS_ERR_UNSUPPORTED;
+    if (!(threshold > 0.0f && threshold < 1.0f) || (bounds != 0 && bounds != 1)) return FGSS_ERR_INVALID;
+    BoundTables b;
+    compute_bounds(threshold, bounds, b);
+    for (uint32_t S = 0; S <= max_sum; S++) {
+        if (cand_min) cand_min[S] = b.cand_min[S];
+        if (inter_min) inter_min[S] = b.inter_min[S];
+    }
+    return FGSS_OK;
+}
+
 fgss_status fgss_dev_exclusive_scan_u32(fgss_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t n) {
     if (!ctx || (n && (!in || !out))) return FGSS_ERR_INVALID;
     return guard(ctx, [&] {

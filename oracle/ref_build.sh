@@ -1,12 +1,18 @@
 #!/bin/bash
-# Builds the reference project's own preprocessing CLI (host C++ only) from its
-# sources where they lie, into oracle/_ref/.  Test infrastructure: the CPU
-# tests run it to pin the tokenizer's token and term counts.  The reference's
-# join is CUDA and is not built or run here.
+# Builds, into oracle/_ref/, test infrastructure from the reference project's
+# own sources where they lie (nothing is copied): the CPU tests run these to pin
+# the oracle and the library against the reference's code.
+#   preprocess   its preprocessing CLI (host C++): token and term counts
+#   ref_bounds   oracle/ref_bounds.cpp over its include/fgssjoin/similarity.cuh,
+#                compiled on the host: the float32 bound tables
+#   ref_load     oracle/ref_load.cu over its src/fgssjoin/data.cu loader
+#                (ppjoin_format, host code only): the .bin record order
+# The reference's join kernels are not run here.
 set -e
 REF=${FGSS_REFERENCE:-/root/reference}  # where the reference checkout lies
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
+NVCC=${NVCC:-/usr/local/cuda/bin/nvcc}
 [ -d "$REF/src" ] || { echo "reference sources not found at $REF; nothing to build"; exit 0; }
 mkdir -p "$OUT"
 g++ -O2 -std=c++11 -w \
@@ -15,3 +21,14 @@ g++ -O2 -std=c++11 -w \
     "$REF/src/preprocess/string/data.cpp" "$REF/src/preprocess/string/qgram.cpp" \
     "$REF/src/io.cpp" "$REF/src/util.cpp" -o "$OUT/preprocess"
 echo "built $OUT/preprocess"
+# strict IEEE float, no FMA contraction: the expressions round as written
+g++ -O2 -std=c++11 -w -fno-fast-math -ffp-contract=off -I"$REF/include/fgssjoin" \
+    "$HERE/ref_bounds.cpp" -o "$OUT/ref_bounds"
+echo "built $OUT/ref_bounds"
+if [ "$HERE/ref_load.cu" -nt "$OUT/ref_load" ] || [ ! -x "$OUT/ref_load" ]; then
+    "$NVCC" -O2 -std=c++14 -w -gencode arch=compute_100a,code=sm_100a \
+        -I"$REF/include" -I"$REF/include/fgssjoin" \
+        "$HERE/ref_load.cu" "$REF/src/fgssjoin/data.cu" "$REF/src/util.cu" "$REF/src/util.cpp" "$REF/src/io.cpp" \
+        -o "$OUT/ref_load" -lcuda
+    echo "built $OUT/ref_load"
+fi
