@@ -1,12 +1,13 @@
 """Benchmark of the set-similarity self-join (one JSON line on stdout).
 
-Workload (default, "titles100k"): 100,000 synthetic title records (5-15 words,
-Zipf(1.1) over a seeded 50,000-word vocabulary, 10 % perturbed copies),
-padded lower-case 3-grams with distinct ids by ascending frequency, self-joined
-at every threshold t in {0.5, 0.6, 0.7, 0.8, 0.9}.  One step = the five joins.
+Workload (default, "heavy1m"): 1,000,000 heavy-tailed records (lognormal word
+counts, mu 2.5, sigma 1.0, 2-600 words drawn Zipf(1.1) from a seeded 50,000-word
+vocabulary, 5 % near-duplicate clusters of 2-20 perturbed copies), padded
+lower-case 3-grams with distinct ids by ascending frequency, self-joined at
+t = 0.7.  One step = that join.
 Other workloads:
-  heavy1m    1,000,000 heavy-tailed records (lognormal word counts, 2-600 words,
-             5 % near-duplicate clusters), t = 0.7;
+  titles100k 100,000 title records (5-15 words, 10 % perturbed copies) self-joined
+             at every t in {0.5, 0.6, 0.7, 0.8, 0.9} (one step = the five joins);
   reads500k  500,000 150-base reads from a seeded 5 Mbp genome (0.5 % substitutions),
              canonical 16-mer sets, t = 0.8;
   batch256   256 independent joins of title records, log-uniform sizes 1,000-200,000,
@@ -19,11 +20,13 @@ Other workloads:
 
 Metric: candidates per second (candidates = the reference's "# Candidates"
 counter, identical for every method) of the batched + learned form; the plain
-per-stage form is timed on the same step and reported beside it, with a check
-that both pair sets are identical.
+per-stage form (same filters, per-stage launches, exact two-pass counts) and
+the batched form without the learned model are timed on the same step and
+reported beside it, device-resident and end to end, with checks that every
+pair set is identical and equal to the CPU oracle's.
 
   python bench.py [--gpus N] [--steps K] [--warmup W]
-                  [--workload titles100k|heavy1m|reads500k|batch256|rs200k|titles18k|heavy300k]
+                  [--workload heavy1m|titles100k|reads500k|batch256|rs200k|titles18k|heavy300k]
                   [--thresholds 0.7,0.9] [--no-model] [--no-tune] [--no-cpu-baseline]
   python bench.py --impl reference ...   # the CPU restatement of the reference algorithm
 """
@@ -41,7 +44,8 @@ sys.path.insert(0, ROOT)
 
 WORKLOADS = {
     "titles100k": dict(kind="titles", n=100_000, seed=2, thresholds=[0.5, 0.6, 0.7, 0.8, 0.9]),
-    "heavy1m": dict(kind="heavy", n=1_000_000, seed=3, thresholds=[0.7]),
+    # ref_step: the reference arm times every ref_step-th query per step (a strided sample)
+    "heavy1m": dict(kind="heavy", n=1_000_000, seed=3, thresholds=[0.7], ref_step=4),
     "reads500k": dict(kind="reads", n=500_000, seed=5, thresholds=[0.8]),
     "batch256": dict(kind="batch", joins=256, lo=1000, hi=200_000, seed=6),
     "rs200k": dict(kind="rs", n=200_000, seed=8, thresholds=[0.6, 0.8]),
@@ -178,21 +182,23 @@ def measured_peaks():
 
 
 def cpu_sample(w, jobs):
-    """The bounded CPU sample of one step: every join of a single-file workload;
-    every 8th join of the 256-join batch (32 joins, about 1/8 of its records)."""
+    """The bounded CPU sample of one step, as job indices: every join of a
+    single-file workload; every 8th join of the 256-join batch (32 joins, about
+    1/8 of its records)."""
     if w["kind"] == "batch":
-        return [j for k, j in enumerate(jobs) if k % 8 == 0]
-    return list(jobs)
+        return [k for k in range(len(jobs)) if k % 8 == 0]
+    return list(range(len(jobs)))
 
 
-def oracle_sets(w, texts, sample):
+def oracle_sets(w, texts, sample, jobs):
     """Memory-order records of the sampled files, tokenized by the oracle."""
     from oracle import oracle as O
     if w["kind"] == "rs":
         (_, rp, rl, rt), (_, sp, sl, stk), nt = O.tokenize_dual(texts[0], texts[1], **tok_opts(w))
         return {0: (rp, rl, rt, nt), 1: (sp, sl, stk, nt)}
     mem = {}
-    for ti, _ in sample:
+    for k in sample:
+        ti = jobs[k][0]
         if ti not in mem:
             ids, lens, tok, loc, nt = O.tokenize(texts[ti], **tok_opts(w))
             _, mpos, mlen, mtok = O.file_to_memory(ids, lens, tok)
@@ -200,34 +206,47 @@ def oracle_sets(w, texts, sample):
     return mem
 
 
-def cpu_reference(w, jobs, mem, steps, warmup):
+def cpu_reference(w, jobs, mem, steps, warmup, q_step=1, keep_pairs=False):
     """The reference algorithm on the host cores (oracle restatement, OpenMP)
     over the bounded sample of one step; ``mem`` maps a file index to its
-    memory-order (pos, len, tokens, n_terms).
-    -> (candidates/s, ms per sample, threads, note)."""
+    memory-order (pos, len, tokens, n_terms).  With q_step > 1 a step joins
+    every q_step-th query only (phase = step number mod q_step), against the
+    whole index.  -> (candidates/s, ms per step, threads, note, {job index:
+    pairs} of the last step when keep_pairs)."""
     from oracle import oracle as O
     sample = cpu_sample(w, jobs)
     threads = O.lib().orc_num_threads()
-    times, cands = [], []
+    times, cands, pairs = [], [], {}
     for it in range(warmup + steps):
+        phase = it % q_step
         t0 = time.perf_counter()
         c = 0
-        for ti, t in sample:
-            mpos, mlen, mtok, nt = mem[ti]
+        for k in sample:
+            ti, t = jobs[k]
             if w["kind"] == "rs":  # R-S join of file 0 (R) with file 1 (S)
-                _, st = O.rsjoin(mem[0][:3], mem[1][:3], nt, t, threads=threads)
+                p, st = O.rsjoin(mem[0][:3], mem[1][:3], mem[0][3], t, threads=threads)
             else:
-                _, st = O.join(mpos, mlen, mtok, nt, t, threads=threads)
+                mpos, mlen, mtok, nt = mem[ti]
+                p, st = O.join(mpos, mlen, mtok, nt, t, threads=threads, query_step=q_step, query_phase=phase)
             c += st["candidates"]
+            if keep_pairs:
+                pairs[k] = p
         dt = time.perf_counter() - t0
         if it >= warmup:
             times.append(dt)
             cands.append(c)
-    recs = sum(len(m[1]) for m in mem.values()) if w["kind"] == "rs" else \
-        sum(len(mem[ti][1]) for ti in {ti for ti, _ in sample})
-    note = ("%d of %d joins (%d records), oracle restatement, OpenMP, %d threads"
-            % (len(sample), len(jobs), recs, threads))
-    return float(np.sum(cands) / np.sum(times)), float(np.mean(times) * 1000.0), threads, note
+    recs = sum(len(m[1]) for m in mem.values())
+    note = ("%d of %d joins (%d records)%s, oracle restatement, OpenMP, %d threads"
+            % (len(sample), len(jobs), recs,
+               ", every %dth query per step" % q_step if q_step > 1 else "", threads))
+    return float(np.sum(cands) / np.sum(times)), float(np.mean(times) * 1000.0), threads, note, pairs
+
+
+def bench_config(args, w, jobs, ws):
+    """The config dict of the JSON line; both arms print the same one."""
+    return {"workload": args.workload, "joins_per_step": len(jobs),
+            "thresholds": sorted({float(t) for _, t in jobs}),
+            "l2": "flushed between steps (256 MB write)", "parallelism": "replicas x%d" % ws}
 
 
 def tok_opts(w):
@@ -244,14 +263,14 @@ def run_reference(args, w):
         return
     _, jobs = workload_jobs(w, only=())
     sample = cpu_sample(w, jobs)
-    texts, _ = workload_jobs(w, only={ti for ti, _ in sample})
-    v, ms, threads, note = cpu_reference(w, jobs, oracle_sets(w, texts, sample), args.steps, args.warmup)
+    texts, _ = workload_jobs(w, only={jobs[k][0] for k in sample})
+    mem = oracle_sets(w, texts, sample, jobs)
+    v, ms, threads, note, _ = cpu_reference(w, jobs, mem, args.steps, args.warmup, q_step=w.get("ref_step", 1))
     line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "candidates/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded generator, see bench.py docstring)",
-            "config": {"workload": args.workload, "joins_per_step": len(jobs),
-                       "thresholds": sorted({t for _, t in jobs})},
+            "config": bench_config(args, w, jobs, ws),
             "cpu_baseline": {"value": v, "unit": "candidates/s", "cores": threads, "kind": "port", "sample": note},
             "e2e": {"value": v, "unit": "candidates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -290,7 +309,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="titles100k", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="heavy1m", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-model", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
@@ -377,10 +396,11 @@ def main():
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
 
-    def step_batched(view_fn):
+    def step_batched(view_fn, model=None):
+        um = use_model if model is None else model
         if w["kind"] == "rs":
-            return [ctx.rsjoin(view_fn(0), view_fn(1), t, method="batched", use_model=use_model) for t in ts]
-        return ctx.selfjoin_batch([view_fn(ti) for ti, _ in jobs], ts, method="batched", use_model=use_model)
+            return [ctx.rsjoin(view_fn(0), view_fn(1), t, method="batched", use_model=um) for t in ts]
+        return ctx.selfjoin_batch([view_fn(ti) for ti, _ in jobs], ts, method="batched", use_model=um)
 
     def step_plain(view_fn, per_join_ms=None):
         """The plain form: the joins one after another, one call each."""
@@ -430,17 +450,26 @@ def main():
         barrier()
         return tot_ms, outs, stats
 
+    def same_pairs(xs, ys):
+        return all(np.array_equal(a.q, b.q) and np.array_equal(a.s, b.s) and np.array_equal(a.overlap, b.overlap)
+                   for a, b in zip(xs, ys))
+
     clocks = Clocks(local)
     bat_ms, bat_out, bat_stats = timed(lambda: step_batched(dev_view), args.steps, args.warmup, "batched_step")
     clk = clocks.stop()
+    # the batched form without the learned model (model-free presizing and work items)
+    nom_ms, nom_out = None, None
+    if use_model:
+        nom_ms, nom_out, _ = timed(lambda: step_batched(dev_view, False), args.steps, args.warmup, "no_model_step")
     plain_steps = max(1, args.steps // 2)
     plain_join_ms = []
     plain_ms, plain_out, _ = timed(lambda: step_plain(dev_view, plain_join_ms), plain_steps, 1, "plain_step")
-    same = all(np.array_equal(a.q, b.q) and np.array_equal(a.s, b.s) and np.array_equal(a.overlap, b.overlap)
-               for a, b in zip(bat_out, plain_out))
     cands = sum(o.stats["candidates"] for o in bat_out)
     # e2e: host (pinned) inputs, H2D + join + D2H of the pairs inside the timed region
     e2e_ms, e2e_out, _ = timed(lambda: step_batched(host_view), args.steps, 1, "e2e_step")
+    plain_e2e_ms, plain_e2e_out, _ = timed(lambda: step_plain(host_view), plain_steps, 1, "plain_e2e_step")
+    same = same_pairs(bat_out, plain_out) and same_pairs(e2e_out, plain_out) and \
+        same_pairs(plain_e2e_out, plain_out) and (nom_out is None or same_pairs(nom_out, plain_out))
     # bytes copied to the device per step: an R-S join copies both files per call; the joins of one
     # batched call that share host arrays copy them once
     def set_bytes(k):
@@ -450,7 +479,6 @@ def main():
     else:
         h2d = sum(set_bytes(k) for k in {ti for ti, _ in jobs})
     d2h = sum(len(o) * 24 for o in e2e_out)
-    same_e2e = all(np.array_equal(a.q, b.q) and np.array_equal(a.s, b.s) for a, b in zip(e2e_out, plain_out))
 
     # per-join latency (the 256-join batch): every join of the batch finishes when the batched call
     # returns; the plain joins finish one after another.  "alone": each join run by itself.
@@ -478,10 +506,12 @@ def main():
                     "sizes_records": _pct([sets[ti].n_sets for ti, _ in jobs])}
 
     # max over ranks
-    vals = torch.tensor([bat_ms, plain_ms, e2e_ms], dtype=torch.float64, device=dev)
+    vals = torch.tensor([bat_ms, plain_ms, e2e_ms, plain_e2e_ms, nom_ms or 0.0], dtype=torch.float64, device=dev)
     if ws > 1:
         torch.distributed.all_reduce(vals, op=torch.distributed.ReduceOp.MAX)
-    bat_ms, plain_ms, e2e_ms = vals.tolist()
+    bat_ms, plain_ms, e2e_ms, plain_e2e_ms, nom_ms_m = vals.tolist()
+    if nom_ms is not None:
+        nom_ms = nom_ms_m
 
     # roofline of the fused filter+verify kernel (one launch per step covers every join of the step)
     last = bat_stats[-1]
@@ -498,29 +528,43 @@ def main():
     launches = int(np.mean([sum(x["launches"] for x in s) if w["kind"] == "rs" else s[0]["launches"]
                             for s in bat_stats]))
 
-    cpu = None
+    cpu, oracle_eq = None, None
     if rank == 0 and not args.no_cpu_baseline:
-        # the same records the GPU joined (the GPU tokenizer's output equals the oracle's)
+        # the same records the GPU joined (the GPU tokenizer's output equals the oracle's), the
+        # whole join once: its rate is the CPU baseline and its pairs are compared with the GPU's
+        sample = cpu_sample(w, jobs)
         mem = {ti: (sets[ti].pos, sets[ti].len, sets[ti].tokens, sets[ti].n_terms)
-               for ti in (range(len(sets)) if w["kind"] == "rs" else {ti for ti, _ in cpu_sample(w, jobs)})}
-        v, ms, threads, note = cpu_reference(w, jobs, mem, 1, 0)
+               for ti in (range(len(sets)) if w["kind"] == "rs" else {jobs[k][0] for k in sample})}
+        v, ms, threads, note, opairs = cpu_reference(w, jobs, mem, 1, 0, keep_pairs=True)
         cpu = {"value": v, "unit": "candidates/s", "cores": threads, "kind": "port", "sample": note}
+        eq = all(np.array_equal(bat_out[k].q, p["q"]) and np.array_equal(bat_out[k].s, p["s"]) and
+                 np.array_equal(bat_out[k].overlap, p["overlap"]) and np.array_equal(bat_out[k].sim, p["sim"])
+                 for k, p in opairs.items())
+        oracle_eq = {"equal": bool(eq), "joins_compared": len(opairs), "joins": len(jobs),
+                     "compared": "q, s, overlap, float similarity (bit-exact)"}
 
     if rank == 0:
         per_step = bat_ms / args.steps
+        plain_step = plain_ms / plain_steps
         uniq = range(len(sets)) if w["kind"] == "rs" else sorted({ti for ti, _ in jobs})
         line = {
             "metric": METRIC,
             "value": ws * cands / (per_step * 1e-3), "unit": "candidates/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator, see bench.py docstring)",
-            "config": {"workload": args.workload, "records": sum(sets[ti].n_sets for ti in uniq),
-                       "tokens": sum(sets[ti].n_tokens for ti in uniq),
-                       "thresholds": t_list, "joins_per_step": len(jobs),
-                       "l2": "flushed between steps (256 MB write)", "parallelism": "replicas x%d" % ws},
-            "plain_ms_per_step": plain_ms / plain_steps,
-            "speedup_vs_plain": (plain_ms / plain_steps) / per_step,
-            "pair_sets_identical": bool(same and same_e2e),
+            "config": bench_config(args, w, jobs, ws),
+            "workload_size": {"records": sum(sets[ti].n_sets for ti in uniq),
+                              "tokens": sum(sets[ti].n_tokens for ti in uniq)},
+            "plain_ms_per_step": plain_step,
+            "plain_e2e_ms_per_step": plain_e2e_ms / plain_steps,
+            "speedup_vs_plain": plain_step / per_step,
+            "speedup_vs_plain_e2e": (plain_e2e_ms / plain_steps) / (e2e_ms / args.steps),
+            "no_model_ms_per_step": nom_ms / args.steps if nom_ms is not None else None,
+            "speedup_vs_plain_no_model": plain_step / (nom_ms / args.steps) if nom_ms is not None else None,
+            "model_speedup": (nom_ms / args.steps) / per_step if nom_ms is not None else None,
+            "plain_method": "same filters as batched (bitmap bound included), per-stage launches, exact two-pass counts",
+            "pair_sets_identical": bool(same),
+            "pairs_equal_oracle": oracle_eq,
             "candidates_per_step": cands, "results_per_step": R,
             "autotune": {t: "%dx%d/rt%d" % (v["threads"], v["hash_log2"], v["regs_rt"]) for t, v in tuned.items()},
             "model": model_report(use_model, model_loss, first_stats[0], bat_stats, len(jobs)),

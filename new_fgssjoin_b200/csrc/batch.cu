@@ -244,9 +244,7 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         uint32_t* pred = c.devT<uint32_t>(J.pfx("pred"), n + 1);
         pre[i] = c.devT<uint64_t>(J.pfx("cpre"), n + 1);
         uint4* meta = c.devT<uint4>(J.pfx("meta"), n + 1);
-        // bitmap filter width: 512 bits when records average more than 96 tokens
-        // (a 256-bit bitmap of a long record is too full to bound much)
-        const uint32_t bmw = J.in.n_tokens > 96ull * std::max<uint64_t>(n, 1) ? 4u : 2u;
+        const uint32_t bmw = bitmap_words(J.in.n_tokens, n);
         uint4* bmap = c.devT<uint4>(J.pfx("bmap"), (uint64_t)bmw * n + 4);
         uint2* qchunk = c.devT<uint2>(J.pfx("qchunk"), n + 1);
         const uint64_t cbuf_cap = 2 * J.in.n_tokens + (1u << 20);  // overflowing queries bisect instead

@@ -145,39 +145,6 @@ static __global__ void k_chunks(JoinArgs a, const uint32_t* __restrict__ poff, c
     }
 }
 
-// Bitmap filter (the bitwise overlap bound of Sandes, Teodoro and Melo for
-// exact set similarity joins): every record's tokens hashed into a bitmap.  A
-// bit set in only one of two bitmaps comes from at least one token in only one
-// of the two records, so |x & y| <= (|x| + |y| - popcount(b(x) ^ b(y))) / 2.
-// Warp per record (a long record's bitmap is nearly full and bounds little,
-// but it is exact, so the bound holds for every pair).  Width: bmw uint4 per
-// record, 2 (256 bits) or 4 (512 bits, for joins of longer records).
-static __global__ void k_bitmaps(JoinArgs a, uint4* __restrict__ bmap, uint32_t bmw) {
-    __shared__ uint32_t sw[8][16];  // launched with 256 threads: a bitmap per warp
-    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t lane = lane_id(), wl = threadIdx.x >> 5;
-    const uint32_t shift = bmw == 4 ? 23 : 24;  // bit index: top 9 or 8 bits of a multiplicative hash
-    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < a.n; r += warps) {
-        if (lane < 16) sw[wl][lane] = 0;
-        __syncwarp();
-        const uint32_t l = a.len[r];
-        const uint32_t* t = a.tok + a.pos[r];
-        for (uint32_t j = lane; j < l; j += 32) {
-            const uint32_t b = (__ldg(t + j) * 0x9E3779B1u) >> shift;
-            atomicOr(&sw[wl][b >> 5], 1u << (b & 31));
-        }
-        __syncwarp();
-        if (lane < bmw)
-            bmap[bmw * r + lane] =
-                make_uint4(sw[wl][4 * lane], sw[wl][4 * lane + 1], sw[wl][4 * lane + 2], sw[wl][4 * lane + 3]);
-        __syncwarp();
-    }
-}
-
-__device__ __forceinline__ uint32_t popc_xor(uint4 a, uint4 b) {
-    return __popc(a.x ^ b.x) + __popc(a.y ^ b.y) + __popc(a.z ^ b.z) + __popc(a.w ^ b.w);
-}
-
 struct FusedArgs {
     const uint32_t* poff;    // per query: first probe window
     const uint2* win;

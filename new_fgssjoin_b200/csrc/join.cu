@@ -310,7 +310,12 @@ void join_plain_filter_verify(Ctx& c, JoinState& J, bool want_cand) {
     // ---- verification (thread-per-candidate merge in the reference; warp per candidate here)
     uint32_t* ov = c.devT<uint32_t>(J.pfx("ov"), C + 1);
     if (C) {
-        k_verify<<<grid_for(C * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(a, cand, d_nc, ov);
+        // token bitmaps of every record (the same filter the batched method uses)
+        const uint32_t bmw = bitmap_words(J.in.n_tokens, n);
+        uint4* bmap = c.devT<uint4>(J.pfx("bmap"), (uint64_t)bmw * n + 4);
+        k_bitmaps<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(a, bmap, bmw);
+        FGSS_LAUNCH_CK();
+        k_verify<<<grid_for(C * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(a, cand, d_nc, ov, bmap, bmw);
         FGSS_LAUNCH_CK();
     }
     // ---- compaction of the verified pairs: count -> scan -> fill

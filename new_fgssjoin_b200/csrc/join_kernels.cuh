@@ -842,13 +842,55 @@ __global__ void __launch_bounds__(NT) k_probe_heavy(const JoinArgs* __restrict__
     }
 }
 
+// Bitmap filter (the bitwise overlap bound of Sandes, Teodoro and Melo for
+// exact set similarity joins): every record's tokens hashed into a bitmap.  A
+// bit set in only one of two bitmaps comes from at least one token in only one
+// of the two records, so |x & y| <= (|x| + |y| - popcount(b(x) ^ b(y))) / 2.
+// Warp per record (a long record's bitmap is nearly full and bounds little,
+// but it is exact, so the bound holds for every pair).  Width: bmw uint4 per
+// record, 2 (256 bits) or 4 (512 bits, for joins of longer records).
+static __global__ void k_bitmaps(JoinArgs a, uint4* __restrict__ bmap, uint32_t bmw) {
+    __shared__ uint32_t sw[8][16];  // launched with 256 threads: a bitmap per warp
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t lane = lane_id(), wl = threadIdx.x >> 5;
+    const uint32_t shift = bmw == 4 ? 23 : 24;  // bit index: top 9 or 8 bits of a multiplicative hash
+    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < a.n; r += warps) {
+        if (lane < 16) sw[wl][lane] = 0;
+        __syncwarp();
+        const uint32_t l = a.len[r];
+        const uint32_t* t = a.tok + a.pos[r];
+        for (uint32_t j = lane; j < l; j += 32) {
+            const uint32_t b = (__ldg(t + j) * 0x9E3779B1u) >> shift;
+            atomicOr(&sw[wl][b >> 5], 1u << (b & 31));
+        }
+        __syncwarp();
+        if (lane < bmw)
+            bmap[bmw * r + lane] =
+                make_uint4(sw[wl][4 * lane], sw[wl][4 * lane + 1], sw[wl][4 * lane + 2], sw[wl][4 * lane + 3]);
+        __syncwarp();
+    }
+}
+
+// Bitmap width of a join in uint4 words: 4 (512 bits) when its records average
+// more than 96 tokens (a 256-bit bitmap of a long record is too full to bound
+// much), else 2 (256 bits).
+inline uint32_t bitmap_words(uint64_t n_tokens, uint64_t n_sets) {
+    return n_tokens > 96ull * (n_sets ? n_sets : 1) ? 4u : 2u;
+}
+
+__device__ __forceinline__ uint32_t popc_xor(uint4 a, uint4 b) {
+    return __popc(a.x ^ b.x) + __popc(a.y ^ b.y) + __popc(a.z ^ b.z) + __popc(a.w ^ b.w);
+}
+
 // ------------------------------------------------- plain verification stage
 
 // Warp per candidate record (q, s, matches, last query position); the source
 // position is found by a search, q tokens are searched in global memory.
 // Writes the overlap (0 when it cannot reach floor(min overlap)).
+// A candidate whose bitmap bound (k_bitmaps) is below floor(min overlap) can
+// be no intersection and skips its merge, as in the batched method's kernel.
 static __global__ void k_verify(JoinArgs a, const uint4* __restrict__ cand, const uint64_t* __restrict__ d_nc,
-                                uint32_t* __restrict__ ov) {
+                                uint32_t* __restrict__ ov, const uint4* __restrict__ bmap, uint32_t bmw) {
     const uint32_t nc = (uint32_t)*d_nc;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t lane = lane_id();
@@ -858,10 +900,16 @@ static __global__ void k_verify(JoinArgs a, const uint4* __restrict__ cand, cons
         const uint32_t q = r.x, s = r.y, c = r.z, jm = r.w;
         const uint32_t lq = a.len[q], ls = a.len[s], S = lq + ls;
         const uint32_t imin = a.inter_min[S];
-        const uint32_t* qt = a.tok + a.pos[q];
-        const uint32_t* st = a.tok + a.pos[s];
-        const uint32_t smx = warp_find(st, a.index[ls], __ldg(qt + jm));
-        const uint32_t o = warp_merge_count(qt, jm + 1, lq, st, smx + 1, ls, c, imin);
+        // lanes 0..bmw-1 each xor one 128-bit word of the two bitmaps
+        uint32_t pc = lane < bmw ? popc_xor(__ldg(bmap + bmw * q + lane), __ldg(bmap + bmw * s + lane)) : 0u;
+        pc = warp_sum(pc);
+        uint32_t o = 0;
+        if (S >= 2 * imin + pc) {
+            const uint32_t* qt = a.tok + a.pos[q];
+            const uint32_t* st = a.tok + a.pos[s];
+            const uint32_t smx = warp_find(st, a.index[ls], __ldg(qt + jm));
+            o = warp_merge_count(qt, jm + 1, lq, st, smx + 1, ls, c, imin);
+        }
         const bool ok = o >= imin && o > 0;
         if (lane == 0) {
             ov[i] = ok ? o : 0;

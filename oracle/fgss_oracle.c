@@ -328,6 +328,9 @@ static void pv_push(pairvec* v, orc_pair x)
  *   side:       NULL, or one byte per record; pairs of records with the same
  *               side byte are skipped before any filter (the R-S join as the
  *               self-join of R and S together restricted to pairs across).
+ *   q_step, q_phase: with q_step > 1 only queries q with (q - q_lo) % q_step
+ *               == q_phase (a strided sample of the queries, keeping their
+ *               size distribution: the bounded CPU baseline of large joins).
  *   want_cands: if nonzero, *cands receives every candidate as
  *               (q, s, partial score) triples -- the cells with score > 0
  *               after filtering (filtering.cu:52-57 / compaction.cu:8-17).
@@ -336,7 +339,7 @@ static void pv_push(pairvec* v, orc_pair x)
 int64_t orc_join(const uint32_t* pos, const uint32_t* len, const uint32_t* tokens,
                  uint32_t n, uint32_t n_terms, float t, uint32_t block_size, int nthreads,
                  orc_pair** out, orc_stats* st, int want_cands, uint32_t** cands, uint64_t* n_cands,
-                 uint32_t q_lo, uint32_t q_hi, const uint8_t* side)
+                 uint32_t q_lo, uint32_t q_hi, const uint8_t* side, uint32_t q_step, uint32_t q_phase)
 {
     if (!(t > 0.0f && t < 1.0f)) return -ORC_ERR_ARG;
     memset(st, 0, sizeof(*st));
@@ -387,6 +390,7 @@ int64_t orc_join(const uint32_t* pos, const uint32_t* len, const uint32_t* token
         const int64_t qb = (q_hi > q_lo) ? (int64_t)(q_hi < n ? q_hi : n) : (int64_t)n;
 #pragma omp for schedule(dynamic, 16)
         for (int64_t qq = qa; qq < qb; qq++) {
+            if (q_step > 1 && (uint32_t)((qq - qa) % q_step) != q_phase) continue;  /* a strided sample */
             uint32_t query = (uint32_t)qq;
             uint32_t jb = query / block_size;          /* query block */
             uint32_t q_offset = jb * block_size;

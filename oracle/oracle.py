@@ -51,7 +51,7 @@ def lib():
         L.orc_join.argtypes = [u32p, u32p, u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
                                ctypes.c_uint32, ctypes.c_int, P(P(_Pair)), P(_Stats), ctypes.c_int,
                                P(u32p), P(ctypes.c_uint64), ctypes.c_uint32, ctypes.c_uint32,
-                               P(ctypes.c_uint8)]
+                               P(ctypes.c_uint8), ctypes.c_uint32, ctypes.c_uint32]
         L.orc_join.restype = ctypes.c_int64
         L.orc_brute.argtypes = [u32p, u32p, u32p, ctypes.c_uint32, ctypes.c_float, P(P(_Pair))]
         L.orc_brute.restype = ctypes.c_int64
@@ -153,8 +153,10 @@ def encode_bin(ids, lens, tokens):
 
 
 def join(pos, lens, tokens, n_terms, t, block_size=0, threads=0, want_candidates=False, query_range=None,
-         side=None):
+         side=None, query_step=1, query_phase=0):
     """Reference-semantics self-join on MEMORY-order records.
+    ``query_step`` > 1 restricts the queries to every query_step-th one (from
+    ``query_phase``): a strided sample for bounded CPU timing.
 
     Returns (pairs, stats[, candidates]) where pairs is a structured array
     (q, s, overlap, sim) sorted by (q, s) in memory indices and stats a dict
@@ -177,7 +179,7 @@ def join(pos, lens, tokens, n_terms, t, block_size=0, threads=0, want_candidates
         side_p = side_a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
     n = L.orc_join(pp, lp, tp, len(len_a), int(n_terms), ctypes.c_float(t), block_size, nthreads,
                    ctypes.byref(out), ctypes.byref(st), int(want_candidates), ctypes.byref(cptr),
-                   ctypes.byref(ncand), int(qb), int(qe), side_p)
+                   ctypes.byref(ncand), int(qb), int(qe), side_p, int(query_step), int(query_phase))
     if n < 0:
         raise ValueError("orc_join failed: %d" % n)
     pairs = _pairs(out, n)
