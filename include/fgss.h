@@ -184,6 +184,7 @@ typedef struct fgss_stats {
     uint64_t launches;        /* kernels launched by the call */
     uint64_t predicted_candidates; /* batched method with use_model: the learned model's estimates */
     uint64_t predicted_results;    /* of candidates and results (0 otherwise; compare with the exact counts) */
+    uint64_t query_tokens;    /* batched method: tokens of the query records the fused kernel staged */
 } fgss_stats;
 
 typedef struct fgss_pairs {

@@ -63,7 +63,8 @@ class _Stats(ctypes.Structure):
                 ("ms_total", ctypes.c_float), ("ms_index", ctypes.c_float), ("ms_filter", ctypes.c_float),
                 ("ms_verify", ctypes.c_float), ("ms_output", ctypes.c_float), ("ms_probe", ctypes.c_float),
                 ("merged_tokens", ctypes.c_uint64), ("launches", ctypes.c_uint64),
-                ("predicted_candidates", ctypes.c_uint64), ("predicted_results", ctypes.c_uint64)]
+                ("predicted_candidates", ctypes.c_uint64), ("predicted_results", ctypes.c_uint64),
+                ("query_tokens", ctypes.c_uint64)]
 
 
 class _Pairs(ctypes.Structure):

@@ -67,6 +67,7 @@ void fill_stats(const JoinState& J, fgss_stats* st) {
     st->heavy_queries = J.stats_host[SS_HEAVY];
     st->overflow_retries = J.overflow_retries;
     st->merged_tokens = J.stats_host[SS_MERGED];
+    st->query_tokens = J.stats_host[SS_QTOK];
     st->predicted_candidates = J.pred_candidates;
     st->predicted_results = J.pred_results;
 }
@@ -823,6 +824,7 @@ fgss_status fgss_selfjoin_to_file(fgss_ctx* ctx, const fgss_sets_view* sets, con
                 total.ms_output += st.ms_output;
                 total.ms_probe += st.ms_probe;
                 total.merged_tokens += st.merged_tokens;
+                total.query_tokens += st.query_tokens;
                 total.launches += st.launches;
                 total.predicted_candidates += st.predicted_candidates;
                 total.predicted_results += st.predicted_results;

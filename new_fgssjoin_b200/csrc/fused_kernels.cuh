@@ -12,15 +12,11 @@
 //   * k_fused: persistent CTAs pull work items (runs of queries of one join,
 //     longest first, claimed one item ahead).  Per query: the query's tokens
 //     and a membership structure (bitmap, hashed set or hashed bitmap) go to
-//     shared memory; per chunk the window entries are accumulated into a
-//     shared-memory slot table (64-bit CAS per entry) that also appends every
-//     newly occupied slot to a list, and a lane-persistent loop drains that
-//     list: each lane takes the next slot, decides whether it is a reference
-//     candidate and whether a merge can still reach floor(min overlap) (by
-//     positions, then by a 256- or 512-bit bitmap bound), then
-//     merges the source's tokens 8 per step against the membership structure,
-//     taking the next slot as soon as it is done; when at most a few merges
-//     remain the warp takes them together, 32 tokens per step.
+//     shared memory; per chunk of its id window the window entries are
+//     accumulated into a shared-memory slot table (64-bit CAS per entry; the
+//     index entry carries the source's size), the occupied slots are decided
+//     from shared memory alone, the bitmap bound of the survivors is checked
+//     with a few lanes per source, and warps merge the few that remain.
 #pragma once
 
 #include "join_kernels.cuh"
@@ -31,10 +27,9 @@ namespace fgss {
 // source position of the last match (11; 2047 = too large to keep) |
 // number of prefix matches (10).
 constexpr uint32_t kSmaxUnknown = 2047;
-// The warp merges together when at most this many of its lanes still merge.
-constexpr uint32_t kCoopMerges = 4;
 
-// Layout: slots u64[H] | occ u16[H] | wlo,whi,clo u32[PC] | wpre u32[PC+4] | qtok u32[QC] | bm u32[BW]
+// Layout: slots u64[H] | occ u16[H] | sls u16[H] | chk u16[H/2] | wlo,whi,clo u32[PC] |
+//         wpre u32[PC+4] | qtok u32[QC] | bm u32[BW] | mlist u16[MC]
 template <int HLOG>
 struct FusedLayout {
     static constexpr uint32_t H = 1u << HLOG;
@@ -44,14 +39,18 @@ struct FusedLayout {
     static constexpr uint32_t PC = H / 4 > 512 ? 512 : (H / 4 > 256 ? H / 4 : 256);
     static constexpr uint32_t QC = H / 2;     // query tokens staged in shared memory (longer: read from HBM)
     static constexpr uint32_t BW = 1024;      // bitmap words: 32768 bits
+    static constexpr uint32_t MC = 512;       // merge list entries per chunk (more: merged by their lane)
     static constexpr size_t off_occ = 8ull * H;
-    static constexpr size_t off_wlo = off_occ + 2ull * H;
+    static constexpr size_t off_sls = off_occ + 2ull * H;   // source size of each slot
+    static constexpr size_t off_chk = off_sls + 2ull * H;   // bitmap-check list (<= one per occupied slot <= cap)
+    static constexpr size_t off_wlo = off_chk + 1ull * H;
     static constexpr size_t off_whi = off_wlo + 4ull * PC;
     static constexpr size_t off_clo = off_whi + 4ull * PC;
     static constexpr size_t off_wpre = off_clo + 4ull * PC;
     static constexpr size_t off_qtok = off_wpre + 4ull * (PC + 4);
     static constexpr size_t off_bm = off_qtok + 4ull * QC;
-    static constexpr size_t bytes = off_bm + 4ull * BW;
+    static constexpr size_t off_ml = off_bm + 4ull * BW;
+    static constexpr size_t bytes = off_ml + 2ull * MC;
     static_assert(off_bm % 16 == 0, "the membership words are cleared with 16-byte stores");
 };
 
@@ -205,21 +204,22 @@ __device__ __forceinline__ void bm_insert(uint32_t* bm, uint32_t mode, uint32_t 
 // are added to the join's 64-bit statistics when the CTA moves to another join
 // (or one of them passes 2^30) and at the end.
 struct FusedCounters {
-    uint32_t cand, inter, res, window, verified, merged;
+    uint32_t cand, inter, res, window, verified, merged, qtok;
 };
 
 // Warp-collective: adds the warp's counters to the join's statistics and clears them.
 __device__ __forceinline__ void flush_fused_counters(const JoinArgs& a, FusedCounters& c) {
-    const unsigned long long v[6] = {warp_sum((unsigned long long)c.cand), warp_sum((unsigned long long)c.inter),
+    const unsigned long long v[7] = {warp_sum((unsigned long long)c.cand), warp_sum((unsigned long long)c.inter),
                                      warp_sum((unsigned long long)c.res), warp_sum((unsigned long long)c.window),
-                                     warp_sum((unsigned long long)c.verified), warp_sum((unsigned long long)c.merged)};
+                                     warp_sum((unsigned long long)c.verified), warp_sum((unsigned long long)c.merged),
+                                     warp_sum((unsigned long long)c.qtok)};
     if (lane_id() == 0) {
-        const int idx[6] = {SS_CANDIDATES, SS_INTERSECTIONS, SS_RESULTS, SS_WINDOW, SS_VERIFIED, SS_MERGED};
+        const int idx[7] = {SS_CANDIDATES, SS_INTERSECTIONS, SS_RESULTS, SS_WINDOW, SS_VERIFIED, SS_MERGED, SS_QTOK};
 #pragma unroll
-        for (int i = 0; i < 6; i++)
+        for (int i = 0; i < 7; i++)
             if (v[i]) atomicAdd(&a.stats[idx[i]], v[i]);
     }
-    c = {0, 0, 0, 0, 0, 0};
+    c = {0, 0, 0, 0, 0, 0, 0};
 }
 
 // One merge step: up to 8 source tokens from position k (two independent
@@ -250,25 +250,60 @@ __device__ __forceinline__ uint32_t merge_step(const uint32_t* __restrict__ st, 
     return hits;
 }
 
+// Counts one candidate whose verification is finished with overlap o.
+__device__ __forceinline__ void tally_overlap(const JoinArgs& a, FusedCounters& ctr, uint32_t q, uint32_t s,
+                                              uint32_t o, uint32_t im, uint32_t need) {
+    if (o >= im && o > 0) {
+        ctr.inter++;
+        if (o >= need) {
+            ctr.res++;
+            emit_result(a, q, s, o);
+        }
+    }
+}
+
 // SIDED: an R-S join (a.side set); self-joins use the instantiation without the side test.
+//
+// Per query: stage its tokens and membership structure, then per chunk of its
+// id window (one chunk when the windows fit the slot table):
+//   1. accumulate: every window entry (source s, query position j, source
+//      position and size from the index entry) goes into the shared slot table
+//      with one 64-bit CAS (key s; match count, last match positions); a
+//      newly occupied slot records the source's size beside it and is appended
+//      to the occupied list (one shared atomic per warp);
+//   2a. decide from shared memory: per occupied slot the reference-candidate
+//      and needs-merge tests read the slot word, the size beside it and the
+//      bound table (no gather per source); slots that need a merge go on the
+//      bitmap-check list;
+//   2b. bitmap bound: bmw lanes per listed source, one 16-byte word each (a
+//      warp loads 8 or 16 bitmaps with one instruction); sources whose bound
+//      can still reach floor(min overlap) go on the merge list;
+//   3. merge: warps take the merge list, 32 source tokens per step (one
+//      coalesced load, a membership test per lane, ballot + popcount), with
+//      the early exit of checking.cu:150-157; slots are cleared meanwhile.
+// Every loop that ballots runs per warp (its bound is the same on all lanes).
 template <int NT, int HLOG, bool SIDED>
 __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, unsigned char* smem,
                             FusedCounters& ctr) {
     using Lay = FusedLayout<HLOG>;
+    constexpr uint32_t NW = NT / 32;
     unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem);
     uint16_t* occ = reinterpret_cast<uint16_t*>(smem + Lay::off_occ);
+    uint16_t* sls = reinterpret_cast<uint16_t*>(smem + Lay::off_sls);
+    uint16_t* chk = reinterpret_cast<uint16_t*>(smem + Lay::off_chk);
     uint32_t* wlo = reinterpret_cast<uint32_t*>(smem + Lay::off_wlo);
     uint32_t* whi = reinterpret_cast<uint32_t*>(smem + Lay::off_whi);
     uint32_t* clo = reinterpret_cast<uint32_t*>(smem + Lay::off_clo);
     uint32_t* wpre = reinterpret_cast<uint32_t*>(smem + Lay::off_wpre);
     uint32_t* qtok = reinterpret_cast<uint32_t*>(smem + Lay::off_qtok);
     uint32_t* bm = reinterpret_cast<uint32_t*>(smem + Lay::off_bm);
-    __shared__ uint32_t s_L, s_sp, s_nocc, s_next, s_cand, s_win;
+    uint16_t* mlist = reinterpret_cast<uint16_t*>(smem + Lay::off_ml);
+    __shared__ uint32_t s_sp, s_nocc, s_nchk, s_nm, s_cand, s_win;
     __shared__ uint4 s_qbm[4];  // the query's bitmap
     __shared__ uint32_t s_sa[48], s_sb[48], s_sc[48];
     __shared__ uint32_t wsum[33];
 
-    const uint32_t tid = threadIdx.x, lane = tid & 31;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const uint32_t st_bits = *a.status;
     if (st_bits & ST_SKIP_ALL) return;
     if (q < a.q_lo || q >= a.q_hi) return;
@@ -280,7 +315,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     const bool unsorted = (st_bits & ST_UNSORTED) != 0;
     const uint32_t send = unsorted ? a.n : a.send[lq];
     if (send <= q + 1) return;
-    if (qp > Lay::PC) {
+    if (qp > Lay::PC || qp >= a.heavy_min_qp) {  // a query of the global-memory accumulator
         if (tid == 0) defer_heavy(a, q);
         return;
     }
@@ -317,30 +352,42 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
         s_cand = 0;
         s_win = 0;
         s_sp = 0;
+        s_nocc = 0;
+        s_nchk = 0;
+        s_nm = 0;
+        ctr.qtok += lq;
+        if (one_chunk) wpre[qp] = qm.w;
     }
+    const uint4* smin = fa.smin + lq;  // indexed by the source size
+    // The chunks of the query's id window: a single chunk when its windows fit
+    // the slot table, else the precomputed split, whose parts bisect
+    // themselves further while they hold more than `cap` entries.  A chunk's
+    // windows are in clo / wpre (wpre[qp] = L entries) before it is
+    // accumulated, decided and merged.
     const uint32_t span = send - q - 1;
-    for (uint32_t ci = 0; ci < nch; ci++) {
-        __syncthreads();
-        if (tid == 0) {
+    const uint32_t n_parts = one_chunk ? 1u : nch;
+    for (uint32_t ci = 0; ci < n_parts; ci++) {
+        __syncthreads();  // the staged query; every thread is done with the chunk stack
+        if (tid == 0 && !one_chunk) {
             // chunk ci of the precomputed split (tag ci: windows from the boundary buffer)
             s_sa[0] = q + 1 + (uint32_t)(((uint64_t)span * ci) / nch);
             s_sb[0] = q + 1 + (uint32_t)(((uint64_t)span * (ci + 1)) / nch);
             s_sc[0] = ci;
             s_sp = 1;
         }
+        bool single_done = false;
         for (;;) {
-            __syncthreads();
-            const uint32_t sp = s_sp;
-            if (sp == 0) break;
-            const uint32_t ra = s_sa[sp - 1], rb = s_sb[sp - 1], tag = s_sc[sp - 1];
+            uint32_t L;
             if (one_chunk) {
-                if (tid == 0) {
-                    wpre[qp] = qm.w;
-                    s_L = qm.w;
-                    s_nocc = 0;
-                    s_next = 0;
-                }
+                if (single_done) break;
+                single_done = true;
+                L = qm.w;
+                if (tid == 0) s_win += L;
             } else {
+                __syncthreads();
+                const uint32_t sp = s_sp;
+                if (sp == 0) break;
+                const uint32_t ra = s_sa[sp - 1], rb = s_sb[sp - 1], tag = s_sc[sp - 1];
                 constexpr uint32_t PER = (Lay::PC + NT - 1) / NT;
                 const uint32_t b0 = tid * PER;
                 uint32_t loc[PER];
@@ -364,222 +411,250 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                     loc[i] = cnt;
                     sum += cnt;
                 }
-                uint32_t tot;
-                uint32_t pre = block_excl_scan<uint32_t>(sum, wsum, &tot);
+                // (its barriers also order every thread's read of the stack top
+                // before thread 0 changes it below)
+                uint32_t pre = block_excl_scan<uint32_t>(sum, wsum, &L);
 #pragma unroll
                 for (uint32_t i = 0; i < PER; i++) {
                     const uint32_t j = b0 + i;
                     if (j < qp) wpre[j] = pre;
                     pre += loc[i];
                 }
+                if (L > Lay::cap && rb - ra > 1) {
+                    if (tid == 0) {  // bisect an oversized range; the lower half first
+                        const uint32_t mid = ra + (rb - ra) / 2;
+                        s_sa[sp - 1] = mid;
+                        s_sb[sp - 1] = rb;
+                        s_sc[sp - 1] = 0xffffffffu;
+                        s_sa[sp] = ra;
+                        s_sb[sp] = mid;
+                        s_sc[sp] = 0xffffffffu;
+                        s_sp = sp + 1;
+                    }
+                    continue;
+                }
                 if (tid == 0) {
-                    wpre[qp] = tot;
-                    s_L = tot;
-                    s_nocc = 0;
-                    s_next = 0;
+                    wpre[qp] = L;
+                    s_sp = sp - 1;
+                    s_win += L;
                 }
-            }
-            __syncthreads();
-            const uint32_t L = s_L;
-            if (L > Lay::cap && rb - ra > 1) {
-                if (tid == 0) {  // bisect an oversized range; the lower half first
-                    const uint32_t mid = ra + (rb - ra) / 2;
-                    s_sa[sp - 1] = mid;
-                    s_sb[sp - 1] = rb;
-                    s_sc[sp - 1] = 0xffffffffu;
-                    s_sa[sp] = ra;
-                    s_sb[sp] = mid;
-                    s_sc[sp] = 0xffffffffu;
-                    s_sp = sp + 1;
-                }
-                continue;
-            }
-            if (tid == 0) {
-                s_sp = sp - 1;
-                s_win += L;
+                if (L == 0) continue;
+                __syncthreads();  // wpre complete
             }
             if (L == 0) continue;
             int hl = 6;
             while ((1u << hl) < 2 * L && hl < HLOG) hl++;
             const uint32_t mask = (1u << hl) - 1;
-            // accumulate; newly occupied slots go on the occupied list.  A thread's
-            // entries f increase, so its token index j only moves forward; four
-            // entries' loads are issued before their slot updates.
+            // 1. accumulate.  A lane's entries f increase, so its token index j
+            // only moves forward; four entries' loads are issued before their
+            // slot updates.
             uint32_t j = 0;
-            for (uint32_t f0 = tid; f0 < L; f0 += 4 * NT) {
-                uint32_t sv[4], jv[4];
+            for (uint32_t f0 = tid - lane; f0 < L; f0 += 4 * NT) {
+                uint32_t sv[4], pv[4], jv[4];
 #pragma unroll
                 for (uint32_t u = 0; u < 4; u++) {
-                    const uint32_t f = f0 + u * NT;
+                    const uint32_t f = f0 + lane + u * NT;
                     sv[u] = kEmpty;
                     if (f < L) {
                         while (wpre[j + 1] <= f) j++;
                         const uint32_t k = clo[j] + (f - wpre[j]);
                         sv[u] = __ldg(a.ent_s + k);
-                        jv[u] = (j << 11) | min((uint32_t)__ldg(a.ent_p + k), kSmaxUnknown);
+                        pv[u] = __ldg(a.ent_pl + k);  // source size << 16 | source position
+                        jv[u] = j;
                     }
                 }
 #pragma unroll
                 for (uint32_t u = 0; u < 4; u++) {
                     const uint32_t s = sv[u];
-                    if (s == kEmpty) continue;
-                    if (unsorted && !size_ok(a, lq, a.len[s])) continue;
-                    if (SIDED && __ldg(sidep + s) == side_q) continue;
-                    const uint32_t pos = jv[u];  // query position << 11 | source position
-                    uint32_t h = hash_slot(s, hl);
-                    bool done = false;
-                    unsigned long long old = kEmptySlot;  // first try assumes an empty slot
-                    for (uint32_t it = 0; it <= mask && !done;) {
-                        const uint32_t key = (uint32_t)(old >> 32);
-                        unsigned long long nw;
-                        if (key == s) {
-                            const uint32_t lo = (uint32_t)old;
-                            // positions of later matches are larger on both sides: keep the max
-                            const uint32_t lastpos = max(lo >> 10, pos);
-                            nw = ((unsigned long long)s << 32) | (lastpos << 10) | ((lo & 0x3ffu) + 1u);
-                        } else if (key == kEmpty) {
-                            nw = ((unsigned long long)s << 32) | (pos << 10) | 1u;
-                        } else {
-                            h = (h + 1) & mask;
-                            it++;
-                            old = *(volatile unsigned long long*)&slots[h];
-                            continue;
-                        }
-                        const unsigned long long prev = atomicCAS(&slots[h], old, nw);
-                        if (prev == old) {
-                            if (key == kEmpty) occ[atomicAdd(&s_nocc, 1u)] = (uint16_t)h;
-                            done = true;
-                        } else {
-                            old = prev;
+                    uint32_t claimed = 0xffffffffu;  // the slot this entry newly occupied
+                    if (s != kEmpty) {
+                        const uint32_t ls = pv[u] >> 16;
+                        bool skip = unsorted && !size_ok(a, lq, ls);
+                        if (SIDED && !skip) skip = __ldg(sidep + s) == side_q;
+                        if (!skip) {
+                            // query position << 11 | source position (2047: too large to keep)
+                            const uint32_t pos = (jv[u] << 11) | min(pv[u] & 0xffffu, kSmaxUnknown);
+                            uint32_t h = hash_slot(s, hl);
+                            bool done = false;
+                            unsigned long long old = kEmptySlot;  // the first try assumes an empty slot
+                            for (uint32_t it = 0; it <= mask && !done;) {
+                                const uint32_t key = (uint32_t)(old >> 32);
+                                unsigned long long nw;
+                                if (key == s) {
+                                    const uint32_t lo = (uint32_t)old;
+                                    // positions of later matches are larger on both sides: keep the max
+                                    const uint32_t lastpos = max(lo >> 10, pos);
+                                    nw = ((unsigned long long)s << 32) | (lastpos << 10) | ((lo & 0x3ffu) + 1u);
+                                } else if (key == kEmpty) {
+                                    nw = ((unsigned long long)s << 32) | (pos << 10) | 1u;
+                                } else {
+                                    h = (h + 1) & mask;
+                                    it++;
+                                    old = *(volatile unsigned long long*)&slots[h];
+                                    continue;
+                                }
+                                const unsigned long long prev = atomicCAS(&slots[h], old, nw);
+                                if (prev == old) {
+                                    if (key == kEmpty) {
+                                        claimed = h;
+                                        sls[h] = (uint16_t)ls;
+                                    }
+                                    done = true;
+                                } else {
+                                    old = prev;
+                                }
+                            }
+                            if (!done) atomicOr(a.status, ST_HASH_FULL);
                         }
                     }
-                    if (!done) atomicOr(a.status, ST_HASH_FULL);
+                    // newly occupied slots onto the occupied list, one shared atomic per warp
+                    const uint32_t m = __ballot_sync(kFull, claimed != 0xffffffffu);
+                    if (m) {
+                        uint32_t base = 0;
+                        if (lane == 0) base = atomicAdd(&s_nocc, (uint32_t)__popc(m));
+                        base = __shfl_sync(kFull, base, 0);
+                        if (claimed != 0xffffffffu) occ[base + __popc(m & lanemask_lt())] = (uint16_t)claimed;
+                    }
                 }
             }
             __syncthreads();
-            // lane-persistent decide + merge over the occupied slots; the whole warp
-            // iterates until every lane has drained the list, and lanes without a
-            // candidate take the next slots with one atomic per warp
+            // 2a. decide from shared memory: reference candidate?  needs a merge?
             const uint32_t nocc = s_nocc;
             uint32_t my_cand = 0;
-            bool have = false, drained = false;
-            uint32_t s = 0, c = 0, xq = 0, ls = 0, k = 0, cnt = 0, qrest = 0, im = 0, need = 0, p0 = 0;
-            const uint32_t* st = nullptr;
-            auto tally = [&](uint32_t o, uint32_t kend) {
-                ctr.verified++;
-                ctr.merged += kend - p0;
-                if (o >= im && o > 0) {
-                    ctr.inter++;
-                    if (o >= need) {
-                        ctr.res++;
-                        emit_result(a, q, s, o);
-                    }
-                }
-            };
-            for (;;) {
-                const uint32_t want = __ballot_sync(kFull, !have && !drained);
-                uint32_t i = 0xffffffffu;
-                if (want) {
-                    const uint32_t leader = __ffs(want) - 1;
-                    uint32_t base = 0;
-                    if (lane == leader) base = atomicAdd(&s_next, (uint32_t)__popc(want));
-                    base = __shfl_sync(kFull, base, leader);
-                    i = base + __popc(want & lanemask_lt());
-                }
-                if (!have && !drained) {
-                    if (i >= nocc) {
-                        drained = true;
+            for (uint32_t i0 = tid - lane; i0 < nocc; i0 += NT) {
+                const uint32_t i = i0 + lane;
+                bool check = false;
+                uint32_t h = 0;
+                if (i < nocc) {
+                    h = occ[i];
+                    const unsigned long long v = slots[h];
+                    const uint32_t s = (uint32_t)(v >> 32), lo = (uint32_t)v;
+                    const uint32_t c = lo & 0x3ffu, jm = lo >> 21, smx = (lo >> 10) & 0x7ffu;
+                    const uint32_t ls = sls[h];
+                    const uint4 sm = __ldg(smin + ls);  // (cand_min, inter_min, need) of |q| + |s|
+                    const uint32_t A = lq - jm;
+                    bool cand, ver;
+                    if (smx != kSmaxUnknown) {
+                        // exact last match on both sides (filtering.cu:127-135 at the last match)
+                        cand = c + min(A, ls - smx) >= sm.x;
+                        ver = c + min(A - 1, ls - smx - 1) >= sm.y;
                     } else {
-                        const unsigned long long v = slots[occ[i]];
-                        s = (uint32_t)(v >> 32);
-                        const uint32_t lo = (uint32_t)v;
-                        c = lo & 0x3ffu;
-                        const uint32_t jm = lo >> 21, smx = (lo >> 10) & 0x7ffu;
                         const uint4 sm4 = fa.meta[s];  // (pos, len, index prefix)
-                        ls = sm4.y;
-                        st = a.tok + sm4.x;
-                        const uint4 sm = fa.smin[lq + ls];
-                        xq = qsrc[jm];
-                        const uint32_t A = lq - jm;
-                        bool cand, ver;
-                        if (smx != kSmaxUnknown) {
-                            // exact last match on both sides (filtering.cu:127-135 at the last match)
-                            cand = c + min(A, ls - smx) >= sm.x;
-                            ver = c + min(A - 1, ls - smx - 1) >= sm.y;
-                        } else {
-                            cand = (c + A >= sm.x) && smax_le(st, (int)ls + (int)c - (int)sm.x, c, sm4.z, xq);
-                            ver = (c + A - 1 >= sm.y) && smax_le(st, (int)ls + (int)c - 1 - (int)sm.y, c, sm4.z, xq);
-                        }
-                        my_cand += cand;
-                        if (ver) {
-                            im = sm.y;
-                            need = sm.z;
-                            qrest = lq - jm - 1;
-                            cnt = c;
-                            // resume right after the last match (or at c when its position was not kept)
-                            k = smx != kSmaxUnknown ? smx + 1 : c;
-                            p0 = k;
-                            if (k >= ls || cnt + min(ls - k, qrest) < im) {
-                                tally(c, k);
-                            } else {
-                                // bitmap bound on the whole overlap: below floor(min overlap), no merge
-                                const uint4* sb = fa.bmap + fa.bmw * s;
-                                uint32_t pc = popc_xor(s_qbm[0], __ldg(sb)) + popc_xor(s_qbm[1], __ldg(sb + 1));
-                                if (fa.bmw == 4) pc += popc_xor(s_qbm[2], __ldg(sb + 2)) + popc_xor(s_qbm[3], __ldg(sb + 3));
-                                if (lq + ls < 2 * im + pc) tally(c, k);
-                                else have = true;
-                            }
-                        }
+                        const uint32_t* st = a.tok + sm4.x;
+                        const uint32_t xq = qsrc[jm];
+                        cand = (c + A >= sm.x) && smax_le(st, (int)ls + (int)c - (int)sm.x, c, sm4.z, xq);
+                        ver = (c + A - 1 >= sm.y) && smax_le(st, (int)ls + (int)c - 1 - (int)sm.y, c, sm4.z, xq);
+                    }
+                    my_cand += cand;
+                    if (ver) {
+                        ctr.verified++;
+                        // the merge resumes right after the last match (or at c when its position
+                        // was not kept); when nothing left can change the count, c is the overlap
+                        const uint32_t k = smx != kSmaxUnknown ? smx + 1 : c;
+                        if (k >= ls || c + min(ls - k, A - 1) < sm.y) tally_overlap(a, ctr, q, s, c, sm.y, sm.z);
+                        else check = true;
                     }
                 }
-                // Nothing left to fetch and at most kCoopMerges merges under way: the
-                // warp takes them one after another, 32 source tokens per step
-                // (one coalesced load, a membership test per lane, ballot +
-                // popcount), with the same early exit as the lane loop.
-                if (__ballot_sync(kFull, !have && !drained) == 0) {
-                    uint32_t act = __ballot_sync(kFull, have);
-                    if (act && __popc(act) <= kCoopMerges) {
-                        while (act) {
-                            const uint32_t l = __ffs(act) - 1;
-                            act &= act - 1;
-                            const uint32_t* wst = reinterpret_cast<const uint32_t*>(
-                                __shfl_sync(kFull, reinterpret_cast<unsigned long long>(st), l));
-                            const uint32_t wls = __shfl_sync(kFull, ls, l), wxq = __shfl_sync(kFull, xq, l);
-                            const uint32_t wc = __shfl_sync(kFull, c, l), wqr = __shfl_sync(kFull, qrest, l);
-                            const uint32_t wim = __shfl_sync(kFull, im, l);
-                            uint32_t wk = __shfl_sync(kFull, k, l), wcnt = __shfl_sync(kFull, cnt, l);
-                            while (wk < wls && wcnt + min(wls - wk, wqr - (wcnt - wc)) >= wim) {
-                                const uint32_t kk = wk + lane;
-                                bool hit = false;
-                                if (kk < wls) {
-                                    const uint32_t x = __ldg(wst + kk);
-                                    hit = x > wxq && bm_test(bm, qmode, x, qsrc, 0, lq);
-                                }
-                                wcnt += __popc(__ballot_sync(kFull, hit));
-                                wk = min(wk + 32u, wls);
-                            }
-                            if (lane == l) {
-                                cnt = wcnt;
-                                k = wk;
-                                have = false;
-                                tally(cnt, k);
-                            }
-                        }
-                    }
+                const uint32_t m = __ballot_sync(kFull, check);
+                if (m) {  // onto the bitmap-check list, one shared atomic per warp
+                    uint32_t base = 0;
+                    if (lane == 0) base = atomicAdd(&s_nchk, (uint32_t)__popc(m));
+                    base = __shfl_sync(kFull, base, 0);
+                    if (check) chk[base + __popc(m & lanemask_lt())] = (uint16_t)h;
                 }
-                if (have) {
-                    cnt += merge_step(st, k, ls, xq, bm, qmode, qsrc, lq);
-                    if (k >= ls || cnt + min(ls - k, qrest - (cnt - c)) < im) {
-                        have = false;
-                        tally(cnt, k);
-                    }
-                }
-                if (__all_sync(kFull, drained)) break;
             }
             my_cand = warp_sum(my_cand);
             if (lane == 0 && my_cand) atomicAdd(&s_cand, my_cand);
             __syncthreads();
+            // 2b. bitmap bound on the whole overlap, bmw lanes per listed source (one
+            // 16-byte word each: a warp loads 32 / bmw bitmaps with one instruction);
+            // a bound below floor(min overlap) means no merge can reach it
+            {
+                const uint32_t nchk = s_nchk, bmw = fa.bmw, G = 32u / bmw;
+                const uint32_t part = lane & (bmw - 1u), grp = lane / bmw;
+                const uint4 qw = s_qbm[part];
+                for (uint32_t e0 = wid * G; e0 < nchk; e0 += NW * G) {
+                    const uint32_t e = e0 + grp;
+                    uint32_t h = 0, pc = 0;
+                    if (e < nchk) {
+                        h = chk[e];
+                        const uint32_t s = (uint32_t)(slots[h] >> 32);
+                        pc = popc_xor(qw, __ldg(fa.bmap + bmw * s + part));
+                    }
+                    pc += __shfl_xor_sync(kFull, pc, 1);
+                    if (bmw == 4) pc += __shfl_xor_sync(kFull, pc, 2);
+                    bool merge = false;
+                    if (e < nchk && part == 0) {
+                        const uint32_t ls = sls[h];
+                        merge = lq + ls >= 2 * __ldg(smin + ls).y + pc;
+                    }
+                    const uint32_t m = __ballot_sync(kFull, merge);
+                    if (m) {  // onto the merge list
+                        uint32_t base = 0;
+                        if (lane == 0) base = atomicAdd(&s_nm, (uint32_t)__popc(m));
+                        base = __shfl_sync(kFull, base, 0);
+                        if (merge) {
+                            const uint32_t mi = base + __popc(m & lanemask_lt());
+                            if (mi < Lay::MC) {
+                                mlist[mi] = (uint16_t)h;
+                            } else {
+                                // the merge list is full: this lane merges the source itself
+                                const unsigned long long v = slots[h];
+                                const uint32_t s = (uint32_t)(v >> 32), lo = (uint32_t)v;
+                                const uint32_t c = lo & 0x3ffu, jm = lo >> 21, smx = (lo >> 10) & 0x7ffu;
+                                const uint32_t ls = sls[h];
+                                const uint4 sm = __ldg(smin + ls);
+                                const uint32_t* st = a.tok + fa.meta[s].x;
+                                const uint32_t xq = qsrc[jm], qrest = lq - jm - 1;
+                                const uint32_t k0 = smx != kSmaxUnknown ? smx + 1 : c;
+                                uint32_t k = k0, cnt = c;
+                                while (k < ls && cnt + min(ls - k, qrest - (cnt - c)) >= sm.y)
+                                    cnt += merge_step(st, k, ls, xq, bm, qmode, qsrc, lq);
+                                ctr.merged += k - k0;
+                                tally_overlap(a, ctr, q, s, cnt, sm.y, sm.z);
+                            }
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            // 3. merge the listed sources (a warp per source) and clear the slots
+            const uint32_t nm = min(s_nm, Lay::MC);
+            for (uint32_t mi = wid; mi < nm; mi += NW) {
+                const uint32_t h = mlist[mi];
+                const unsigned long long v = slots[h];
+                const uint32_t s = (uint32_t)(v >> 32), lo = (uint32_t)v;
+                const uint32_t c = lo & 0x3ffu, jm = lo >> 21, smx = (lo >> 10) & 0x7ffu;
+                const uint32_t ls = sls[h];
+                const uint4 sm = __ldg(smin + ls);
+                const uint32_t im = sm.y;
+                const uint32_t* st = a.tok + fa.meta[s].x;
+                const uint32_t xq = qsrc[jm], qrest = lq - jm - 1;
+                const uint32_t k0 = smx != kSmaxUnknown ? smx + 1 : c;
+                uint32_t k = k0, cnt = c;
+                while (k < ls && cnt + min(ls - k, qrest - (cnt - c)) >= im) {
+                    const uint32_t kk = k + lane;
+                    bool hit = false;
+                    if (kk < ls) {
+                        const uint32_t x = __ldg(st + kk);
+                        hit = x > xq && bm_test(bm, qmode, x, qsrc, 0, lq);
+                    }
+                    cnt += __popc(__ballot_sync(kFull, hit));
+                    k = min(k + 32u, ls);
+                }
+                if (lane == 0) {
+                    ctr.merged += k - k0;
+                    tally_overlap(a, ctr, q, s, cnt, im, sm.z);
+                }
+            }
+            __syncthreads();  // the merges read the slots
             for (uint32_t i2 = tid; i2 < nocc; i2 += NT) slots[occ[i2]] = kEmptySlot;
+            if (tid == 0) {
+                s_nocc = 0;
+                s_nchk = 0;
+                s_nm = 0;
+            }
+            __syncthreads();
         }
     }
     __syncthreads();
@@ -613,7 +688,7 @@ __global__ void __launch_bounds__(NT, RT / NT) k_fused(const JoinArgs* __restric
     for (uint32_t h = threadIdx.x; h < Lay::H; h += NT) slots[h] = kEmptySlot;
     for (uint32_t i = threadIdx.x; i < Lay::BW; i += NT) bm[i] = 0u;
     __syncthreads();
-    FusedCounters ctr = {0, 0, 0, 0, 0, 0};
+    FusedCounters ctr = {0, 0, 0, 0, 0, 0, 0};
     // work items are claimed one ahead: thread 0 claims the next item as the
     // current one starts, so one barrier per item publishes it
     __shared__ uint32_t s_item[2];

@@ -141,6 +141,7 @@ void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_o
     a.heavy_count = J.status + 2;
     a.heavy_cap = (uint32_t)n;
     a.join_id = (uint32_t)slot;
+    a.heavy_min_qp = 0xffffffffu;  // set by the batched method's launch shape
     if (o.query_end > o.query_begin) {
         if (o.query_end > n) fail(FGSS_ERR_INVALID, "query_end beyond the number of records");
         a.q_lo = (uint32_t)o.query_begin;
@@ -179,10 +180,10 @@ void join_index(Ctx& c, JoinState& J) {
     uint32_t* e32 = c.devT<uint32_t>(J.pfx("E32"), 2);
     uint32_t* list_off = c.devT<uint32_t>(J.pfx("list_off"), (uint64_t)J.in.n_terms + 2);
     uint32_t* ent_s = c.devT<uint32_t>(J.pfx("ent_s"), T + 1);
-    uint16_t* ent_p = c.devT<uint16_t>(J.pfx("ent_p"), T + 1);
+    uint32_t* ent_pl = c.devT<uint32_t>(J.pfx("ent_pl"), T + 1);
     a.list_off = list_off;
     a.ent_s = ent_s;
-    a.ent_p = ent_p;
+    a.ent_pl = ent_pl;
     if (n == 0) {
         FGSS_CK(cudaMemsetAsync(list_off, 0, ((uint64_t)J.in.n_terms + 1) * 4, c.stream));
         FGSS_CK(cudaMemsetAsync(J.d_e, 0, 8, c.stream));
@@ -198,7 +199,7 @@ void join_index(Ctx& c, JoinState& J) {
     FGSS_LAUNCH_CK();
     radix_sort<uint32_t, uint64_t>(c, key, val, T, J.d_e, 0, J.term_bits, J.pfx("ixsort").c_str());
     k_index_lists<<<grid_for(T, 256, c.num_sms * 32), 256, 0, c.stream>>>(key, val, J.d_e, J.in.n_terms, list_off,
-                                                                         ent_s, ent_p);
+                                                                         ent_s, ent_pl);
     FGSS_LAUNCH_CK();
 }
 

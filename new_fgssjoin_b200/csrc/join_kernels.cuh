@@ -52,6 +52,7 @@ enum {
     SS_HEAVY,
     SS_PROBE,
     SS_MERGED,
+    SS_QTOK,   // tokens of the query records the fused kernel staged
     SS_N
 };
 
@@ -76,7 +77,7 @@ struct JoinArgs {
     // inverted index
     const uint32_t* list_off;  // [n_terms + 1]
     const uint32_t* ent_s;     // source record of each entry, ascending within a list
-    const uint16_t* ent_p;     // position of the token in the source
+    const uint32_t* ent_pl;    // source size << 16 | position of the token in the source
     // plain method
     uint32_t* vcnt;            // count pass: per query, candidates that need a merge
     uint32_t* ccnt;            // count pass: per query, candidates (reference definition)
@@ -96,7 +97,7 @@ struct JoinArgs {
     uint32_t join_id;
     uint32_t q_lo;             // queries processed: [q_lo, q_hi) (a shard of the join)
     uint32_t q_hi;
-    uint32_t pad_;
+    uint32_t heavy_min_qp;     // fused method: probe prefixes this long go to the global accumulator
     // R-S join: one byte per record (0 = R, 1 = S); pairs within one side are
     // skipped before any filter.  nullptr for a self-join.
     const uint8_t* side;
@@ -241,7 +242,7 @@ static __global__ void k_send(const uint32_t* __restrict__ len, uint32_t n, cons
 
 // -------------------------------------------------------------- index stage
 
-// Index entries of every record's index prefix: key = term, value = record << 16 | position.
+// Index entries of every record's index prefix: key = term, value = record << 32 | size << 16 | position.
 static __global__ void k_index_entries(JoinArgs a, const uint32_t* __restrict__ ioff, uint32_t* __restrict__ key,
                                 uint64_t* __restrict__ val) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -253,7 +254,7 @@ static __global__ void k_index_entries(JoinArgs a, const uint32_t* __restrict__ 
         uint32_t o = ioff[i];
         for (uint32_t j = lane_id(); j < ip; j += 32) {
             key[o + j] = t[j];
-            val[o + j] = ((uint64_t)i << 16) | j;
+            val[o + j] = ((uint64_t)i << 32) | (l << 16) | j;
         }
     }
 }
@@ -262,7 +263,7 @@ static __global__ void k_index_entries(JoinArgs a, const uint32_t* __restrict__ 
 // term boundary fills the offsets of the terms it spans) and the SoA split.
 static __global__ void k_index_lists(const uint32_t* __restrict__ key, const uint64_t* __restrict__ val,
                               const uint64_t* __restrict__ d_e, uint32_t n_terms, uint32_t* __restrict__ list_off,
-                              uint32_t* __restrict__ ent_s, uint16_t* __restrict__ ent_p) {
+                              uint32_t* __restrict__ ent_s, uint32_t* __restrict__ ent_pl) {
     const uint32_t E = (uint32_t)*d_e;
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -272,8 +273,8 @@ static __global__ void k_index_lists(const uint32_t* __restrict__ key, const uin
     }
     for (uint32_t k = tid; k < E; k += stride) {
         uint64_t v = val[k];
-        ent_s[k] = (uint32_t)(v >> 16);
-        ent_p[k] = (uint16_t)(v & 0xffffu);
+        ent_s[k] = (uint32_t)(v >> 32);
+        ent_pl[k] = (uint32_t)v;
         uint32_t w = key[k];
         if (k == 0)
             for (uint32_t x = 0; x <= w; x++) list_off[x] = 0;
@@ -771,7 +772,7 @@ __global__ void __launch_bounds__(NT) k_probe_heavy(const JoinArgs* __restrict__
             uint32_t j = upper_bound_gen(wpre, 0, qp, f) - 1;
             uint32_t k = wlo[j] + (f - wpre[j]);
             uint32_t s = __ldg(a.ent_s + k);
-            uint32_t sp = __ldg(a.ent_p + k);
+            uint32_t sp = __ldg(a.ent_pl + k) & 0xffffu;
             if (unsorted && !size_ok(a, lq, a.len[s])) continue;
             if (a.side && __ldg(a.side + s) == __ldg(a.side + q)) continue;
             uint32_t old = atomicAdd(&gcnt[s], 1u);
