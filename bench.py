@@ -356,7 +356,7 @@ def main():
         d_arrays.append([torch.from_numpy(a.view(np.int32)).to(dev) for a in (s.id, s.pos, s.len, s.tokens)])
         pinned = [torch.from_numpy(a.view(np.int32)).pin_memory() for a in (s.id, s.pos, s.len, s.tokens)]
         host_sets.append(F.Sets(*(p.numpy().view(np.uint32) for p in pinned), n_terms=s.n_terms))
-    del texts, tokenized
+    del tokenized  # (the texts stay for the text-to-pairs leg)
 
     def dev_view(ti):
         v = _View()
@@ -468,8 +468,22 @@ def main():
     # e2e: host (pinned) inputs, H2D + join + D2H of the pairs inside the timed region
     e2e_ms, e2e_out, _ = timed(lambda: step_batched(host_view), args.steps, 1, "e2e_step")
     plain_e2e_ms, plain_e2e_out, _ = timed(lambda: step_plain(host_view), plain_steps, 1, "plain_e2e_step")
+
+    def step_text():
+        """Text in host memory to pairs in host memory: GPU tokenizer, then the
+        batched join of the tokenized records (the user's whole path)."""
+        if w["kind"] == "rs":
+            r, s_ = ctx.tokenize_dual(texts[0], texts[1], **to)
+            return [ctx.rsjoin(r, s_, t, method="batched", use_model=use_model) for t in ts]
+        tok = [ctx.tokenize(x, **to) for x in texts]
+        return ctx.selfjoin_batch([tok[ti] for ti, _ in jobs], ts, method="batched", use_model=use_model)
+
+    text_steps = max(1, args.steps // 2)
+    text_ms, text_out, _ = timed(step_text, text_steps, 1, "text_e2e_step")
+    text_bytes = sum(len(x) for x in texts)
     same = same_pairs(bat_out, plain_out) and same_pairs(e2e_out, plain_out) and \
-        same_pairs(plain_e2e_out, plain_out) and (nom_out is None or same_pairs(nom_out, plain_out))
+        same_pairs(plain_e2e_out, plain_out) and (nom_out is None or same_pairs(nom_out, plain_out)) and \
+        same_pairs(text_out, plain_out)
     # bytes copied to the device per step: an R-S join copies both files per call; the joins of one
     # batched call that share host arrays copy them once
     def set_bytes(k):
@@ -506,10 +520,11 @@ def main():
                     "sizes_records": _pct([sets[ti].n_sets for ti, _ in jobs])}
 
     # max over ranks
-    vals = torch.tensor([bat_ms, plain_ms, e2e_ms, plain_e2e_ms, nom_ms or 0.0], dtype=torch.float64, device=dev)
+    vals = torch.tensor([bat_ms, plain_ms, e2e_ms, plain_e2e_ms, nom_ms or 0.0, text_ms], dtype=torch.float64,
+                        device=dev)
     if ws > 1:
         torch.distributed.all_reduce(vals, op=torch.distributed.ReduceOp.MAX)
-    bat_ms, plain_ms, e2e_ms, plain_e2e_ms, nom_ms_m = vals.tolist()
+    bat_ms, plain_ms, e2e_ms, plain_e2e_ms, nom_ms_m, text_ms = vals.tolist()
     if nom_ms is not None:
         nom_ms = nom_ms_m
 
@@ -522,7 +537,10 @@ def main():
     W = sum(s["window_entries"] for s in last)
     M = sum(s["merged_tokens"] for s in last)
     R = sum(s["results"] for s in last)
-    alg_bytes = 12 * P + 8 * W + 4 * M + 12 * R
+    Q = sum(s["query_tokens"] for s in last)
+    # probe tokens + their list bounds, window entries (source, size|position), merged source
+    # tokens, results, and the query records' tokens staged in shared memory
+    alg_bytes = 12 * P + 8 * W + 4 * M + 12 * R + 4 * Q
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (kern_ms * 1e-3) / 1e9 if kern_ms > 0 else 0.0
     launches = int(np.mean([sum(x["launches"] for x in s) if w["kind"] == "rs" else s[0]["launches"]
@@ -566,14 +584,22 @@ def main():
             "pair_sets_identical": bool(same),
             "pairs_equal_oracle": oracle_eq,
             "candidates_per_step": cands, "results_per_step": R,
+            "counters": {"probe_tokens": P, "window_entries": W, "merged_tokens": M, "query_tokens": Q,
+                         "verified": sum(s["verified"] for s in last), "results": R,
+                         "heavy_queries": sum(s["heavy_queries"] for s in last)},
             "autotune": {t: "%dx%d/rt%d" % (v["threads"], v["hash_log2"], v["regs_rt"]) for t, v in tuned.items()},
             "model": model_report(use_model, model_loss, first_stats[0], bat_stats, len(jobs)),
             "e2e": {"value": ws * cands / (e2e_ms / args.steps * 1e-3), "unit": "candidates/s",
                     "ms_per_step": e2e_ms / args.steps, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e_text": {"value": ws * cands / (text_ms / text_steps * 1e-3), "unit": "candidates/s",
+                         "ms_per_step": text_ms / text_steps, "text_bytes_per_step": text_bytes,
+                         "path": "text in host memory -> GPU tokenizer -> batched join -> pairs in host memory"},
             "roofline": {"bound": "hbm", "kernel": "k_fused", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": profiled_traffic(args.workload), "traffic_source": "profiles/k_fused_%s.md"
-                         % args.workload, "alg_bytes": alg_bytes, "kernel_ms": kern_ms},
+                         % args.workload, "alg_bytes": alg_bytes,
+                         "alg_bytes_formula": "12 probe_tokens + 8 window_entries + 4 merged_tokens + 12 results"
+                                              " + 4 query_tokens", "kernel_ms": kern_ms},
             "gpu_launches": launches * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,
