@@ -69,3 +69,44 @@ def test_streamed_output_file(tmp_path):
                        "--shards", "3", "--method", "batched"])
     assert none == [] and len(lines) > 0
     assert out.read_text().splitlines() == lines and cnt2 == cnt
+
+
+PRE = os.path.join(os.path.dirname(CLI), "preprocess")
+
+
+def test_preprocess_selfjoin_writes_the_reference_fixture(tmp_path):
+    """`preprocess selfjoin small.txt 3` (the reference's command) prints its
+    counts and writes the reference's own fixture files byte for byte."""
+    src = tmp_path / "small.txt"
+    src.write_bytes(open(os.path.join(GOLDEN, "small.txt"), "rb").read())
+    p = subprocess.run([PRE, "selfjoin", str(src), "3"], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    assert "Number of tokens: 88" in p.stdout and "Number of terms: 42" in p.stdout
+    assert (tmp_path / "small.txt.3gram.bin").read_bytes() == \
+        open(os.path.join(GOLDEN, "small.txt.3gram.bin"), "rb").read()
+    assert (tmp_path / "small.txt.3gram.bin.loc").read_bytes() == \
+        open(os.path.join(GOLDEN, "small.txt.3gram.bin.loc"), "rb").read()
+    # and the join reads what it wrote
+    lines, _ = _run([str(tmp_path / "small.txt.3gram.bin"), "0.7"])
+    assert sorted(lines) == json.load(open(os.path.join(GOLDEN, "small_pairs.json")))["0.7"]
+
+
+def test_preprocess_dualjoin_writes_both_files_over_one_vocabulary(tmp_path):
+    """dualjoin tokenizes both files over one vocabulary (document frequency over
+    both) and writes each as a .bin in file order, equal to the oracle's."""
+    text_r, text_s = split_titles(2000, 31)
+    fr, fs = tmp_path / "r.txt", tmp_path / "s.txt"
+    fr.write_bytes(text_r)
+    fs.write_bytes(text_s)
+    p = subprocess.run([PRE, "dualjoin", str(fr), str(fs), "3", "--pad", "--distinct"], capture_output=True,
+                       text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    r, s, nt = oracle_dual(text_r, text_s, **datagen.TITLE_TOK)
+    assert "Number of terms: %d" % nt in p.stdout
+    for path, (ids, pos, lens, toks) in ((fr, r), (fs, s)):
+        order = range(len(ids))[::-1]  # file order: memory order reversed
+        want = (np.asarray(ids)[::-1], np.asarray(lens)[::-1],
+                np.concatenate([toks[pos[i]:pos[i] + lens[i]] for i in order]))
+        got = O.decode_bin(open(str(path) + ".3gram.bin", "rb").read())
+        for g, w_ in zip(got, want):
+            assert np.array_equal(g, np.asarray(w_, dtype=np.uint32))
