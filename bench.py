@@ -29,6 +29,7 @@ pair set is identical and equal to the CPU oracle's.
                   [--workload heavy1m|titles100k|reads500k|batch256|rs200k|titles18k|heavy300k]
                   [--thresholds 0.7,0.9] [--no-model] [--no-tune] [--no-cpu-baseline]
   python bench.py --impl reference ...   # the CPU restatement of the reference algorithm
+  torchrun ... bench.py --gpus N --shard  # one join split over N GPUs by the cost model (strong scaling)
 """
 import argparse
 import json
@@ -276,6 +277,102 @@ def run_reference(args, w):
     print(json.dumps(line), flush=True)
 
 
+def run_sharded(args, w):
+    """--shard: ONE join of the workload split over the ranks by query ranges of
+    equal estimated work (the batched method's cost estimates, computed on rank
+    0 and broadcast), each rank joining its range against the replicated index,
+    then an all-gather of the pair buffers over NCCL (the one exchange).  Every
+    rank holds the same records (the same seed).  Timed: the local joins and the
+    gather, max over ranks; strong scaling (total work fixed)."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    import new_fgssjoin_b200 as F
+    from new_fgssjoin_b200.binding import _View
+    from new_fgssjoin_b200.shard import agreed_ranges, gather_pairs, FIELDS
+    ws, rank, local = dist_env()
+    if w["kind"] not in ("titles", "heavy", "reads"):
+        raise SystemExit("--shard takes a single-file workload")
+    text = make_text(w)  # every rank: the same records
+    t = w["thresholds"][0]
+    train = [make_text(w, seed_offset=7919 + k, n=max(1000, w["n"] // d)) for k, d in enumerate((27, 9, 3))]
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    ctx = F.Context(device=local, stream=stream.cuda_stream)
+    to = tok_opts(w)
+    sets = ctx.tokenize(text, **to)
+    del text
+    ctx.model_train([ctx.tokenize(x, **to) for x in train], [t] * len(train), epochs=300, lr=0.01, seed=1)
+    d = [torch.from_numpy(a.view(np.int32)).to(dev) for a in (sets.id, sets.pos, sets.len, sets.tokens)]
+    v = _View()
+    v.id, v.pos, v.len, v.tokens = [x.data_ptr() for x in d]
+    v.n_sets, v.n_tokens, v.n_terms, v.on_device = sets.n_sets, sets.n_tokens, sets.n_terms, 1
+    if ws > 1:
+        ranges = agreed_ranges(sets.len, ws, lambda: ctx.query_costs(v, t, use_model=True))
+    else:
+        ranges = [(0, int(sets.n_sets))]
+    qr = ranges[rank]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        p = ctx.selfjoin(v, t, method="batched", use_model=True, query_range=qr)
+        cols = {f: getattr(p, f) for f in FIELDS}
+        return p, (gather_pairs(cols) if ws > 1 else cols)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    clocks = Clocks(local)
+    tot = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        p, full = step()
+        e1.record(stream)
+        e1.synchronize()
+        tot += e0.elapsed_time(e1)
+    clk = clocks.stop()
+    barrier()
+    mine = torch.tensor([float(p.stats["candidates"]), float(p.stats["window_entries"])], dtype=torch.float64,
+                        device=dev)
+    if ws > 1:
+        mx = torch.tensor([tot], dtype=torch.float64, device=dev)
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        tot = mx.item()
+        parts = [torch.zeros_like(mine) for _ in range(ws)]
+        dist.all_gather(parts, mine)
+        per_rank = [x.tolist() for x in parts]
+    else:
+        per_rank = [mine.tolist()]
+    if rank == 0:
+        per_step = tot / args.steps
+        cands_all = int(sum(x[0] for x in per_rank))
+        line = {"metric": METRIC, "value": cands_all / (per_step * 1e-3), "unit": "candidates/s", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "int32",
+                "data": "synthetic (seeded generator, see bench.py docstring)",
+                "config": {"workload": args.workload, "joins_per_step": 1, "thresholds": [t],
+                           "l2": "flushed between steps (256 MB write)",
+                           "parallelism": "query-range shards x%d (cost-model balanced), all-gather of pairs" % ws},
+                "results_per_step": len(full["q"]), "candidates_per_step": cands_all,
+                "shard_ranges": ranges, "shard_window_entries": [x[1] for x in per_rank], "clocks": clk}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        dist.destroy_process_group()
+
+
 def model_report(used, loss, first, timed, n_joins):
     """The learned model's error against the exact counts of the same joins, and
     how often its presized result buffers overflowed (an exact re-run each)."""
@@ -313,6 +410,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-model", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--shard", action="store_true", help="one join split over the GPUs (strong scaling)")
     ap.add_argument("--thresholds", type=str, default=None, help="comma-separated, overrides the workload's")
     args = ap.parse_args()
     w = dict(WORKLOADS[args.workload])
@@ -320,6 +418,8 @@ def main():
         w["thresholds"] = [float(x) for x in args.thresholds.split(",")]
     if args.impl == "reference":
         return run_reference(args, w)
+    if args.shard:
+        return run_sharded(args, w)
 
     ws, rank, local = dist_env()
     # record files (untimed) are generated before the first GPU call

@@ -216,6 +216,16 @@ fgss_status fgss_selfjoin_batch(fgss_ctx* ctx, const fgss_sets_view* sets, const
 
 void fgss_pairs_free(fgss_pairs* p);
 
+/* Per-query work estimates of one join, for splitting its queries (the first
+ * records of pairs) over GPUs: costs[q] (n_sets values, host memory) = the
+ * window entries of q's probe prefix + 4 x the learned model's predicted
+ * candidates of q (opts->use_model and a trained model) + |q|, the cost the
+ * batched method balances its work items by.  Runs the index build and the
+ * batched pre-pass on the device.  No reference counterpart (the reference
+ * runs on device 0 only, src/fgssjoin_cli.cu:81). */
+fgss_status fgss_query_costs(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_join_opts* opts,
+                             uint64_t* costs);
+
 /* Formats pairs as the reference prints them: "%d %d %f\n" per pair
  * (block.cu:193).  Writes to the FILE* given as a void* (stdout if NULL). */
 fgss_status fgss_pairs_print(const fgss_pairs* p, void* file);

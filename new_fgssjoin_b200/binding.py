@@ -19,7 +19,7 @@ EXPORTED_SYMBOLS = [
     "fgss_join_opts_default", "fgss_selfjoin", "fgss_selfjoin_batch", "fgss_rsjoin", "fgss_pairs_free",
     "fgss_pairs_print", "fgss_selfjoin_to_file",
     "fgss_model_train", "fgss_model_save", "fgss_model_load", "fgss_model_grad", "fgss_model_num_params",
-    "fgss_autotune", "fgss_bounds_table", "fgss_overlap_table", "fgss_dev_exclusive_scan_u32", "fgss_dev_sort_pairs_u64",
+    "fgss_autotune", "fgss_bounds_table", "fgss_overlap_table", "fgss_query_costs", "fgss_dev_exclusive_scan_u32", "fgss_dev_sort_pairs_u64",
     "fgss_dev_exclusive_scan_u32_noalloc",
 ]
 
@@ -119,6 +119,7 @@ def load_library():
     L.fgss_selfjoin_to_file.argtypes = [ctypes.c_void_p, P(_View), P(_JoinOpts), ctypes.c_char_p, ctypes.c_int,
                                         ctypes.c_int, P(_Stats)]
     L.fgss_pairs_free.argtypes = [P(_Pairs)]
+    L.fgss_query_costs.argtypes = [ctypes.c_void_p, P(_View), P(_JoinOpts), ctypes.c_void_p]
     L.fgss_model_train.argtypes = [ctypes.c_void_p, P(_View), P(ctypes.c_float), ctypes.c_int, ctypes.c_int,
                                    ctypes.c_float, ctypes.c_uint64, P(ctypes.c_float)]
     L.fgss_model_save.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
@@ -374,6 +375,16 @@ class Context:
                     _stats_dict(st), cands)
         L.fgss_pairs_free(ctypes.byref(p))
         return out
+
+    def query_costs(self, sets, threshold, bounds="reference", use_model=True):
+        """Per-query work estimates of the join (fgss_query_costs): window entries
+        + 4 x the learned model's predicted candidates + size, memory order."""
+        v = sets.view() if isinstance(sets, Sets) else sets
+        o = self._opts(threshold, "batched", bounds, False, use_model)
+        out = np.zeros(max(int(v.n_sets), 1), np.uint64)
+        rc = self._L.fgss_query_costs(self._ctx, ctypes.byref(v), ctypes.byref(o), out.ctypes.data)
+        _check(self._L, self._ctx, rc)
+        return out[:int(v.n_sets)]
 
     def selfjoin(self, sets, threshold, method="plain", bounds="reference", want_candidates=False,
                  use_model=False, result_capacity=0, query_range=None):

@@ -919,6 +919,21 @@ fgss_status fgss_bounds_table(float threshold, int bounds, uint32_t max_len, uin
     return FGSS_OK;
 }
 
+fgss_status fgss_query_costs(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_join_opts* opts,
+                             uint64_t* costs) {
+    if (!ctx || !sets || !opts || (!costs && sets->n_sets)) return FGSS_ERR_INVALID;
+    return guard(ctx, [&] {
+        Ctx& c = ctx->c;
+        FGSS_CK(cudaSetDevice(c.device));
+        fgss_join_opts o = *opts;
+        o.query_begin = o.query_end = 0;  // every query gets its estimate
+        JoinState J;
+        join_setup(c, J, *sets, o, 0);
+        join_index(c, J);
+        join_query_costs(c, J, o.use_model != 0, costs);
+    });
+}
+
 fgss_status fgss_overlap_table(float threshold, int bounds, uint32_t max_sum, uint32_t* cand_min,
                                uint32_t* inter_min) {
     if (max_sum > 2 * kMaxLen) return FGSS_ERR_UNSUPPORTED;

@@ -201,6 +201,79 @@ __global__ void k_clear_filter_state(uint32_t* status, unsigned long long* stats
     if (threadIdx.x < SS_N && threadIdx.x != SS_PROBE) stats[threadIdx.x] = 0;
 }
 
+// The batched method's pre-pass of one join (index built already): windows of
+// every probe token (exact per-query work), bitmaps, chunk splits for slot
+// tables of cap_entries, the learned model's estimates (use_model), and the
+// work-item cost of every query (window entries + 4 x predicted candidates +
+// size) with its exclusive prefix in `pre` and total in d_total.
+FusedArgs join_prepass(Ctx& c, JoinState& J, uint32_t cap_entries, bool use_model, uint64_t* d_pred_res,
+                       uint64_t* d_pred_cand, uint64_t* pre, uint64_t* d_total) {
+    const uint64_t n = J.in.n_sets;
+    float* feat = c.devT<float>(J.pfx("feat"), (n + 1) * kFeat);
+    uint64_t* cost = c.devT<uint64_t>(J.pfx("cost"), n + 1);
+    uint32_t* fcost = c.devT<uint32_t>(J.pfx("fcost"), n + 1);
+    uint32_t* poff = c.devT<uint32_t>(J.pfx("poff"), n + 1);
+    uint2* win = c.devT<uint2>(J.pfx("win"), J.in.n_tokens + 1);
+    uint32_t* wpre = c.devT<uint32_t>(J.pfx("wpre"), J.in.n_tokens + 1);
+    uint32_t* wtot = c.devT<uint32_t>(J.pfx("wtot"), n + 1);
+    uint32_t* pred = c.devT<uint32_t>(J.pfx("pred"), n + 1);
+    uint4* meta = c.devT<uint4>(J.pfx("meta"), n + 1);
+    const uint32_t bmw = bitmap_words(J.in.n_tokens, n);
+    uint4* bmap = c.devT<uint4>(J.pfx("bmap"), (uint64_t)bmw * n + 4);
+    uint2* qchunk = c.devT<uint2>(J.pfx("qchunk"), n + 1);
+    const uint64_t cbuf_cap = 2 * J.in.n_tokens + (1u << 20);  // overflowing queries bisect instead
+    uint32_t* cbuf = c.devT<uint32_t>(J.pfx("cbuf"), cbuf_cap);
+    FusedArgs f;
+    f.poff = poff;
+    f.win = win;
+    f.wpre = wpre;
+    f.smin = J.lut.smin;
+    f.meta = meta;
+    f.qchunk = qchunk;
+    f.cbuf = cbuf;
+    f.bmap = bmap;
+    f.bmw = bmw;
+    J.d_cost = cost;
+    if (n == 0) return f;
+    // windows of every probe token (exact per-query work), chunk splits, then
+    // features and the learned estimate, then the work-item cost prefix
+    exclusive_scan<uint32_t>(c, J.pcnt, poff, n, nullptr, (uint32_t*)nullptr, J.pfx("scan.p").c_str());
+    unsigned long long* cused = reinterpret_cast<unsigned long long*>(J.status + 4);
+    FGSS_CK(cudaMemsetAsync(cused, 0, 8, c.stream));
+    k_windows<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wpre, wtot, meta);
+    FGSS_LAUNCH_CK();
+    k_bitmaps<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, bmap, bmw);
+    FGSS_LAUNCH_CK();
+    k_chunks<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wtot, cap_entries, qchunk,
+                                                                        cbuf, cbuf_cap, cused);
+    FGSS_LAUNCH_CK();
+    const bool model = use_model && c.model && !J.res_cap_hint;
+    if (model) {
+        k_features<<<grid_for(n * 32, 256, c.num_sms * 32), 256, 0, c.stream>>>(J.args, J.t, feat, fcost);
+        FGSS_LAUNCH_CK();
+        model_predict(c, feat, n, pred, d_pred_res, d_pred_cand);
+    }
+    k_cost<<<grid_for(n, 256, c.num_sms * 8), 256, 0, c.stream>>>(wtot, J.in.len, model ? pred : nullptr, (uint32_t)n,
+                                                                   J.args.q_lo, J.args.q_hi, cost);
+    FGSS_LAUNCH_CK();
+    exclusive_scan<uint64_t>(c, cost, pre, n, nullptr, d_total, J.pfx("scan.cost").c_str());
+    return f;
+}
+
+// Per-query work estimates of one join (index built already), to host `out`:
+// the costs the batched method balances its work items by.
+void join_query_costs(Ctx& c, JoinState& J, bool use_model, uint64_t* out) {
+    const uint64_t n = J.in.n_sets;
+    if (n == 0) return;
+    const TuneEntry te = tune_lookup(c, tune_key(n, J.in.n_tokens, J.t));
+    uint64_t* d_tot = c.devT<uint64_t>(J.pfx("qc.tot"), 4);
+    FGSS_CK(cudaMemsetAsync(d_tot, 0, 32, c.stream));
+    uint64_t* pre = c.devT<uint64_t>(J.pfx("cpre"), n + 1);
+    join_prepass(c, J, (1u << te.hash_log2) / 2, use_model, d_tot + 1, d_tot + 2, pre, d_tot);
+    FGSS_CK(cudaMemcpyAsync(out, J.d_cost, n * 8, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+}
+
 // Runs the fused filter+verify over every join (their index built already).
 //
 // With a plan in record mode the host-side decisions of this run (launch
@@ -233,54 +306,8 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
     const uint32_t cap_entries = (1u << te.hash_log2) / 2;  // chunk capacity of the chosen kernel shape
     for (size_t i = 0; i < nj; i++) {
         JoinState& J = *joins[i];
-        const uint64_t n = J.in.n_sets;
-        float* feat = c.devT<float>(J.pfx("feat"), (n + 1) * kFeat);
-        uint64_t* cost = c.devT<uint64_t>(J.pfx("cost"), n + 1);
-        uint32_t* fcost = c.devT<uint32_t>(J.pfx("fcost"), n + 1);
-        uint32_t* poff = c.devT<uint32_t>(J.pfx("poff"), n + 1);
-        uint2* win = c.devT<uint2>(J.pfx("win"), J.in.n_tokens + 1);
-        uint32_t* wpre = c.devT<uint32_t>(J.pfx("wpre"), J.in.n_tokens + 1);
-        uint32_t* wtot = c.devT<uint32_t>(J.pfx("wtot"), n + 1);
-        uint32_t* pred = c.devT<uint32_t>(J.pfx("pred"), n + 1);
-        pre[i] = c.devT<uint64_t>(J.pfx("cpre"), n + 1);
-        uint4* meta = c.devT<uint4>(J.pfx("meta"), n + 1);
-        const uint32_t bmw = bitmap_words(J.in.n_tokens, n);
-        uint4* bmap = c.devT<uint4>(J.pfx("bmap"), (uint64_t)bmw * n + 4);
-        uint2* qchunk = c.devT<uint2>(J.pfx("qchunk"), n + 1);
-        const uint64_t cbuf_cap = 2 * J.in.n_tokens + (1u << 20);  // overflowing queries bisect instead
-        uint32_t* cbuf = c.devT<uint32_t>(J.pfx("cbuf"), cbuf_cap);
-        hf[i].poff = poff;
-        hf[i].win = win;
-        hf[i].wpre = wpre;
-        hf[i].smin = J.lut.smin;
-        hf[i].meta = meta;
-        hf[i].qchunk = qchunk;
-        hf[i].cbuf = cbuf;
-        hf[i].bmap = bmap;
-        hf[i].bmw = bmw;
-        if (n == 0) continue;
-        // windows of every probe token (exact per-query work), chunk splits, then
-        // features and the learned estimate, then the work-item cost prefix
-        exclusive_scan<uint32_t>(c, J.pcnt, poff, n, nullptr, (uint32_t*)nullptr, J.pfx("scan.p").c_str());
-        unsigned long long* cused = reinterpret_cast<unsigned long long*>(J.status + 4);
-        FGSS_CK(cudaMemsetAsync(cused, 0, 8, c.stream));
-        k_windows<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wpre, wtot, meta);
-        FGSS_LAUNCH_CK();
-        k_bitmaps<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, bmap, bmw);
-        FGSS_LAUNCH_CK();
-        k_chunks<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wtot, cap_entries,
-                                                                            qchunk, cbuf, cbuf_cap, cused);
-        FGSS_LAUNCH_CK();
-        const bool model = use_model && c.model && !J.res_cap_hint;
-        if (model) {
-            k_features<<<grid_for(n * 32, 256, c.num_sms * 32), 256, 0, c.stream>>>(J.args, J.t, feat, fcost);
-            FGSS_LAUNCH_CK();
-            model_predict(c, feat, n, pred, &d_tot[nj + i], &d_tot[2 * nj + i]);
-        }
-        k_cost<<<grid_for(n, 256, c.num_sms * 8), 256, 0, c.stream>>>(wtot, J.in.len, model ? pred : nullptr,
-                                                                       (uint32_t)n, J.args.q_lo, J.args.q_hi, cost);
-        FGSS_LAUNCH_CK();
-        exclusive_scan<uint64_t>(c, cost, pre[i], n, nullptr, &d_tot[i], J.pfx("scan.cost").c_str());
+        pre[i] = c.devT<uint64_t>(J.pfx("cpre"), J.in.n_sets + 1);
+        hf[i] = join_prepass(c, J, cap_entries, use_model, &d_tot[nj + i], &d_tot[2 * nj + i], pre[i], &d_tot[i]);
     }
     FusedArgs* d_fargs = c.devT<FusedArgs>(c.bpfx + "b.fargs", nj);
     FGSS_CK(cudaMemcpyAsync(d_fargs, hf, nj * sizeof(FusedArgs), cudaMemcpyHostToDevice, c.stream));

@@ -56,6 +56,7 @@ struct JoinState {
     std::vector<uint32_t> cand_host;  // (q, s, partial) triples when requested
     uint64_t pred_results = 0;        // the learned model's estimates (batched method, 0 without it)
     uint64_t pred_candidates = 0;
+    uint64_t* d_cost = nullptr;       // batched pre-pass: per-query work estimates
     std::string ns;                   // buffer-name namespace ("" or a captured graph's own "g<id>.")
     std::string pfx(const char* name) const { return ns + "j" + std::to_string(slot) + "." + name; }
 };
@@ -97,6 +98,8 @@ struct BatchPlan {
     std::vector<uint32_t> heavy_slots;
 };
 void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_model, BatchPlan* plan = nullptr);
+// Per-query work estimates of one join (its index built), copied to host `out` (n values).
+void join_query_costs(Ctx& c, JoinState& J, bool use_model, uint64_t* out);
 
 // Autotuner (tune.cu): workload class of a join, the shapes to try, the
 // cache file.

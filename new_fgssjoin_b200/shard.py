@@ -2,11 +2,16 @@
 
 Every rank holds the whole record set and builds the same inverted index
 (read-only, replicated); the queries -- the first record of each pair -- are
-split into contiguous memory-index ranges of equal estimated work, each rank
-joins its range (``Context.selfjoin(..., query_range=...)``), and the only
-exchange is a final gather of the pair buffers: counts first, then the
-padded payloads.  Ranges are ascending, so concatenating the gathered shards
-in rank order keeps the pairs sorted by (q, s).
+split into contiguous memory-index ranges of equal work, each rank joins its
+range (``Context.selfjoin(..., query_range=...)``), and the only exchange is
+a final gather of the pair buffers: counts first, then the padded payloads.
+Ranges are ascending, so concatenating the gathered shards in rank order
+keeps the pairs sorted by (q, s).
+
+Work per query: by default the batched method's own estimate
+(``Context.query_costs``: exact window entries + 4 x the learned model's
+predicted candidates + size), computed on rank 0, whose cuts are broadcast so
+every rank agrees; without a context, a size-squared proxy.
 """
 import numpy as np
 
@@ -17,12 +22,13 @@ def query_costs(lens):
     return lens * lens + 1.0
 
 
-def shard_ranges(lens, world):
-    """Contiguous query ranges [b, e) of about equal estimated work, one per rank."""
+def shard_ranges(lens, world, costs=None):
+    """Contiguous query ranges [b, e) of about equal estimated work, one per
+    rank; ``costs`` (per query) overrides the size-squared proxy."""
     n = len(lens)
     if world <= 1 or n == 0:
         return [(0, n)] * max(1, world)
-    c = np.cumsum(query_costs(lens))
+    c = np.cumsum(np.asarray(costs, dtype=np.float64) if costs is not None else query_costs(lens))
     total = c[-1]
     cuts = [0]
     for r in range(1, world):
@@ -60,10 +66,32 @@ def gather_pairs(local, group=None):
     return out
 
 
-def sharded_selfjoin(ctx, sets, threshold, rank, world, group=None, method="batched", gather=True):
-    """This rank's shard of the join; with ``gather`` every rank gets the full, sorted result."""
-    qb, qe = shard_ranges(sets.len, world)[rank]
-    local = ctx.selfjoin(sets, threshold, method=method, query_range=(qb, qe))
+def agreed_ranges(lens, world, costs_fn=None, group=None):
+    """Query ranges every rank agrees on: rank 0 computes them (from
+    ``costs_fn()`` when given, else the size proxy) and broadcasts the cuts."""
+    import torch
+    import torch.distributed as dist
+    if world <= 1:
+        return [(0, len(lens))]
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else torch.device("cpu")
+    cuts = torch.zeros(world + 1, dtype=torch.int64, device=dev)
+    if dist.get_rank(group) == 0:
+        r = shard_ranges(lens, world, costs_fn() if costs_fn else None)
+        cuts.copy_(torch.tensor([b for b, _ in r] + [r[-1][1]], dtype=torch.int64))
+    dist.broadcast(cuts, src=0, group=group)
+    c = cuts.tolist()
+    return [(c[i], c[i + 1]) for i in range(world)]
+
+
+def sharded_selfjoin(ctx, sets, threshold, rank, world, group=None, method="batched", gather=True, use_model=True,
+                     ranges=None):
+    """This rank's shard of the join, its queries split by the batched method's
+    cost estimate; with ``gather`` every rank gets the full, sorted result.
+    ``ranges``: query ranges agreed earlier (agreed_ranges), to reuse."""
+    if ranges is None:
+        ranges = agreed_ranges(sets.len, world, lambda: ctx.query_costs(sets, threshold, use_model=use_model), group)
+    qb, qe = ranges[rank]
+    local = ctx.selfjoin(sets, threshold, method=method, query_range=(qb, qe), use_model=use_model)
     if not gather:
         return local
     cols = {f: getattr(local, f) for f in FIELDS}

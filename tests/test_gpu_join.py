@@ -279,6 +279,30 @@ def test_query_range_shards_reassemble_the_join(ctx, titles_sets, method):
     assert sum(p.stats["intersections"] for p in parts) == st["intersections"]
 
 
+def test_query_costs_are_the_batched_work_estimates(ctx, titles_sets):
+    """Without the model a query's cost is its window entries plus its size: the
+    costs sum to the batched join's window-entry counter plus the record sizes."""
+    s = titles_sets
+    cost = ctx.query_costs(s, 0.7, use_model=False)
+    got = ctx.selfjoin(s, 0.7, method="batched")
+    assert len(cost) == s.n_sets and cost.dtype == np.uint64
+    assert int(cost.sum()) == got.stats["window_entries"] + int(s.len.astype(np.uint64).sum())
+
+
+def test_cost_balanced_shards_reassemble_the_join(ctx, titles_sets):
+    """Query ranges cut by the learned cost estimates (as on several GPUs) give the full join."""
+    from new_fgssjoin_b200.shard import shard_ranges
+    s = titles_sets
+    ctx.model_train([s], [0.7], epochs=50, lr=0.01, seed=3)
+    cost = ctx.query_costs(s, 0.7, use_model=True)
+    ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, 0.7)
+    parts = [ctx.selfjoin(s, 0.7, method="batched", query_range=r, use_model=True)
+             for r in shard_ranges(s.len, 4, cost)]
+    assert np.array_equal(np.concatenate([p.q for p in parts]), ref["q"])
+    assert np.array_equal(np.concatenate([p.s for p in parts]), ref["s"])
+    assert sum(p.stats["candidates"] for p in parts) == st["candidates"]
+
+
 def _device_view(sets):
     import torch
     from new_fgssjoin_b200.binding import _View

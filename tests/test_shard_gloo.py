@@ -11,7 +11,7 @@ import pytest
 import torch.multiprocessing as mp
 
 from new_fgssjoin_b200 import datagen
-from new_fgssjoin_b200.shard import gather_pairs, shard_ranges
+from new_fgssjoin_b200.shard import agreed_ranges, gather_pairs, shard_ranges
 from oracle import oracle as O
 
 
@@ -23,12 +23,24 @@ def _free_port():
     return p
 
 
+def _cost_on_rank0_only(rank, mlen):
+    """A per-query cost only rank 0 may compute (as the library's cost model
+    runs on rank 0): any other rank calling it fails the test."""
+    def f():
+        assert rank == 0, "costs computed on a rank other than 0"
+        return np.asarray(mlen, dtype=np.float64) ** 3
+    return f
+
+
 def _worker(rank, world, port, data, t, q):
     import torch.distributed as dist
     dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world)
     try:
         mid, mpos, mlen, mtok, nt = data
-        qb, qe = shard_ranges(mlen, world)[rank]
+        # the cost partition: rank 0's cuts, broadcast (each rank's join stands in for the GPU's)
+        ranges = agreed_ranges(mlen, world, _cost_on_rank0_only(rank, mlen))
+        assert ranges == shard_ranges(mlen, world, np.asarray(mlen, dtype=np.float64) ** 3)
+        qb, qe = ranges[rank]
         pairs, st = O.join(mpos, mlen, mtok, nt, t, query_range=(qb, qe))
         local = {"q": pairs["q"], "s": pairs["s"], "id_q": mid[pairs["q"]], "id_s": mid[pairs["s"]],
                  "overlap": pairs["overlap"], "sim": pairs["sim"]}
