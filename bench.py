@@ -687,7 +687,8 @@ def main():
             "counters": {"probe_tokens": P, "window_entries": W, "merged_tokens": M, "query_tokens": Q,
                          "verified": sum(s["verified"] for s in last), "results": R,
                          "heavy_queries": sum(s["heavy_queries"] for s in last)},
-            "autotune": {t: "%dx%d/rt%d" % (v["threads"], v["hash_log2"], v["regs_rt"]) for t, v in tuned.items()},
+            "autotune": {t: "%s %dx%d/rt%d" % (v["filter"], v["threads"], v["hash_log2"], v["regs_rt"])
+                         for t, v in tuned.items()},
             "model": model_report(use_model, model_loss, first_stats[0], bat_stats, len(jobs)),
             "e2e": {"value": ws * cands / (e2e_ms / args.steps * 1e-3), "unit": "candidates/s",
                     "ms_per_step": e2e_ms / args.steps, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

@@ -147,6 +147,14 @@ enum { FGSS_BOUNDS_REFERENCE = 0, /* float32 bounds exactly as similarity.cuh:9-
        FGSS_BOUNDS_EXACT = 1 };   /* exact rational bounds of the decimal threshold */
 enum { FGSS_METHOD_PLAIN = 0,     /* per-stage launches, exact two-pass counts */
        FGSS_METHOD_BATCHED = 1 }; /* persistent fused kernel, learned presizing, CUDA graph */
+/* Filter strategies of the batched method (its candidate generation +
+ * verification); every one gives the same pairs and counters.  The
+ * reference's live filter is a thread per query (src/fgssjoin/filtering.cu:76-141);
+ * its dead variants a CTA per query (filtering.cu:300-407). */
+enum { FGSS_FILTER_AUTO = 0,      /* the autotuner's choice for the join's workload class */
+       FGSS_FILTER_WARP = 1,      /* fused kernel, one warp per query (32-thread CTAs, small slot table) */
+       FGSS_FILTER_CTA = 2,       /* fused kernel, one 128-thread CTA per query (large slot table) */
+       FGSS_FILTER_GLOBAL = 3 };  /* every query on the dense global-memory accumulator kernel */
 
 typedef struct fgss_join_opts {
     float threshold;        /* Jaccard threshold in (0, 1) (fgssjoin_cli.cu:31-35) */
@@ -160,6 +168,7 @@ typedef struct fgss_join_opts {
     uint64_t query_begin;   /* only queries (first records of pairs) in [query_begin, query_end) */
     uint64_t query_end;     /* are processed; 0, 0 = all.  Used to shard one join over GPUs. */
     int no_graph;           /* batched method on device inputs: 1 = never capture / replay a CUDA graph */
+    int filter;             /* batched method: FGSS_FILTER_* */
 } fgss_join_opts;
 
 void fgss_join_opts_default(fgss_join_opts* o);
@@ -254,10 +263,13 @@ typedef struct fgss_tune_result {
     int ctas_per_sm;   /* resident CTAs per SM (0 = as many as fit) */
     float ms;          /* best filter+verify time measured (device) */
     char key[64];      /* workload class the choice is cached under */
+    int filter;        /* the winning strategy: FGSS_FILTER_WARP / _CTA / _GLOBAL */
 } fgss_tune_result;
 
-/* Times every launch shape of the batched method's fused kernel on this join
- * (reps runs each, best kept) and caches the fastest for its workload class
+/* Times every filter strategy of the batched method on this join -- each launch
+ * shape of the fused kernel (one warp or one CTA per query) and the dense
+ * global-memory accumulator for every query -- (reps runs each, best kept)
+ * and caches the fastest for its workload class
  * (threshold, record-count and average-size buckets), in the context and in
  * the JSON file of fgss_options.tune_cache_path when one was given.  Later
  * batched joins of the same class use it.  No reference counterpart. */

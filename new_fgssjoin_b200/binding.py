@@ -9,6 +9,9 @@ _LIB = os.path.join(_HERE, "_lib", "libfgss.so")
 
 METHOD_PLAIN, METHOD_BATCHED = 0, 1
 BOUNDS_REFERENCE, BOUNDS_EXACT = 0, 1
+# filter strategies of the batched method (fgss_join_opts.filter)
+FILTERS = {"auto": 0, "warp": 1, "cta": 2, "global": 3}
+FILTER_NAMES = {v: k for k, v in FILTERS.items()}
 TOK_QGRAM, TOK_KMER = 0, 1
 
 # every entry point include/fgss.h declares
@@ -52,7 +55,7 @@ class _JoinOpts(ctypes.Structure):
     _fields_ = [("threshold", ctypes.c_float), ("bounds", ctypes.c_int), ("method", ctypes.c_int),
                 ("out_on_device", ctypes.c_int), ("want_candidates", ctypes.c_int), ("use_model", ctypes.c_int),
                 ("result_capacity", ctypes.c_uint64), ("query_begin", ctypes.c_uint64),
-                ("query_end", ctypes.c_uint64), ("no_graph", ctypes.c_int)]
+                ("query_end", ctypes.c_uint64), ("no_graph", ctypes.c_int), ("filter", ctypes.c_int)]
 
 
 class _Stats(ctypes.Structure):
@@ -76,7 +79,7 @@ class _Pairs(ctypes.Structure):
 class _TuneResult(ctypes.Structure):
     _fields_ = [("threads", ctypes.c_int), ("hash_log2", ctypes.c_int), ("regs_rt", ctypes.c_int),
                 ("ctas_per_sm", ctypes.c_int),
-                ("ms", ctypes.c_float), ("key", ctypes.c_char * 64)]
+                ("ms", ctypes.c_float), ("key", ctypes.c_char * 64), ("filter", ctypes.c_int)]
 
 
 class FgssError(RuntimeError):
@@ -347,8 +350,9 @@ class Context:
     # ----------------------------------------------------------------- join
     @staticmethod
     def _opts(threshold, method, bounds, want_candidates, use_model, out_on_device=False, result_capacity=0,
-              query_range=None):
+              query_range=None, filter="auto"):
         o = _JoinOpts()
+        o.filter = FILTERS[filter] if isinstance(filter, str) else int(filter)
         o.threshold = float(threshold)
         o.method = {"plain": METHOD_PLAIN, "batched": METHOD_BATCHED}.get(method, method)
         o.bounds = {"reference": BOUNDS_REFERENCE, "exact": BOUNDS_EXACT}.get(bounds, bounds)
@@ -387,14 +391,14 @@ class Context:
         return out[:int(v.n_sets)]
 
     def selfjoin(self, sets, threshold, method="plain", bounds="reference", want_candidates=False,
-                 use_model=False, result_capacity=0, query_range=None):
+                 use_model=False, result_capacity=0, query_range=None, filter="auto"):
         """Self-join of ``sets`` (host Sets or a device view) at ``threshold``.
 
         ``query_range`` = (begin, end) processes only the pairs whose first
         record (memory index) lies in [begin, end): one shard of the join."""
         v = sets.view() if isinstance(sets, Sets) else sets
         o = self._opts(threshold, method, bounds, want_candidates, use_model, result_capacity=result_capacity,
-                       query_range=query_range)
+                       query_range=query_range, filter=filter)
         p = _Pairs()
         st = _Stats()
         rc = self._L.fgss_selfjoin(self._ctx, ctypes.byref(v), ctypes.byref(o), ctypes.byref(p), ctypes.byref(st))
@@ -428,11 +432,12 @@ class Context:
         return _stats_dict(st)
 
     def selfjoin_batch(self, sets_list, thresholds, method="batched", bounds="reference", use_model=False,
-                       result_capacity=0):
+                       result_capacity=0, filter="auto"):
         """Many independent self-joins in one call (one persistent launch per stage)."""
         n = len(sets_list)
         views = (_View * n)(*[s.view() if isinstance(s, Sets) else s for s in sets_list])
-        opts = (_JoinOpts * n)(*[self._opts(t, method, bounds, False, use_model, result_capacity=result_capacity)
+        opts = (_JoinOpts * n)(*[self._opts(t, method, bounds, False, use_model, result_capacity=result_capacity,
+                                            filter=filter)
                                  for t in thresholds])
         outs = (_Pairs * n)()
         sts = (_Stats * n)()
@@ -448,8 +453,7 @@ class Context:
         _check(self._L, self._ctx, self._L.fgss_autotune(self._ctx, ctypes.byref(v), ctypes.byref(o), reps,
                                                          ctypes.byref(r)))
         return {"threads": r.threads, "hash_log2": r.hash_log2, "regs_rt": r.regs_rt, "ctas_per_sm": r.ctas_per_sm,
-                "ms": r.ms,
-                "key": r.key.decode()}
+                "ms": r.ms, "key": r.key.decode(), "filter": FILTER_NAMES[r.filter]}
 
     # --------------------------------------------------------------- model
     def model_train(self, sets_list, thresholds, epochs=300, lr=0.01, seed=0):

@@ -206,11 +206,11 @@ std::string graph_key(const fgss_sets_view* sets, const fgss_join_opts* opts, in
     for (int i = 0; i < n; i++) {
         uint32_t tb;
         memcpy(&tb, &opts[i].threshold, 4);
-        snprintf(buf, sizeof buf, "%p,%p,%p,%p,%llu,%llu,%u|%u,%d,%d,%llu,%llu,%llu;", (const void*)sets[i].id,
+        snprintf(buf, sizeof buf, "%p,%p,%p,%p,%llu,%llu,%u|%u,%d,%d,%llu,%llu,%llu,%d;", (const void*)sets[i].id,
                  (const void*)sets[i].pos, (const void*)sets[i].len, (const void*)sets[i].tokens,
                  (unsigned long long)sets[i].n_sets, (unsigned long long)sets[i].n_tokens, sets[i].n_terms, tb,
                  opts[i].bounds, opts[i].use_model, (unsigned long long)opts[i].result_capacity,
-                 (unsigned long long)opts[i].query_begin, (unsigned long long)opts[i].query_end);
+                 (unsigned long long)opts[i].query_begin, (unsigned long long)opts[i].query_end, opts[i].filter);
         k += buf;
     }
     return k;
@@ -856,14 +856,19 @@ fgss_status fgss_autotune(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_
         o.method = FGSS_METHOD_BATCHED;
         o.want_candidates = 0;
         o.out_on_device = 1;
+        o.filter = FGSS_FILTER_AUTO;
         const std::string key = tune_key(sets->n_sets, sets->n_tokens, o.threshold);
         TuneEntry win;
         win.ms = 1e30f;
-        for (int i = 0; i < kNumFusedShapes; i++) {
-            TuneEntry te;
-            te.threads = kFusedShapes[i][0];
-            te.hash_log2 = kFusedShapes[i][1];
-            te.regs_rt = kFusedShapes[i][2];
+        // every fused-kernel shape, then every query on the global accumulator
+        for (int i = 0; i <= kNumFusedShapes; i++) {
+            TuneEntry te = filter_entry(FGSS_FILTER_GLOBAL);
+            if (i < kNumFusedShapes) {
+                te.threads = kFusedShapes[i][0];
+                te.hash_log2 = kFusedShapes[i][1];
+                te.regs_rt = kFusedShapes[i][2];
+                te.heavy_min_probe = 0;
+            }
             te.ctas_per_sm = 0;
             c.tune_force = &te;
             float bestms = 1e30f;
@@ -881,8 +886,8 @@ fgss_status fgss_autotune(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_
             }
             c.tune_force = nullptr;
             if (c.verbose)
-                fprintf(stderr, "[fgss] autotune %s: threads %d hash_log2 %d regs_rt %d -> %.3f ms\n", key.c_str(),
-                        te.threads, te.hash_log2, te.regs_rt, bestms);
+                fprintf(stderr, "[fgss] autotune %s: threads %d hash_log2 %d regs_rt %d global %d -> %.3f ms\n",
+                        key.c_str(), te.threads, te.hash_log2, te.regs_rt, te.heavy_min_probe, bestms);
             if (bestms < win.ms) {
                 win = te;
                 win.ms = bestms;
@@ -898,6 +903,7 @@ fgss_status fgss_autotune(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_
             best->ctas_per_sm = win.ctas_per_sm;
             best->ms = win.ms;
             snprintf(best->key, sizeof best->key, "%s", key.c_str());
+            best->filter = filter_of(win);
         }
     });
 }

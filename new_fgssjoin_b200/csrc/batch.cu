@@ -151,6 +151,22 @@ extern const int kFusedShapes[][3] = {{32, 8, 1024},  {32, 9, 1024},  {64, 9, 10
                                       {128, 11, 768}, {256, 11, 768}};
 extern const int kNumFusedShapes = 10;
 
+// The launch shape that stands for a requested filter strategy.
+TuneEntry filter_entry(int filter) {
+    TuneEntry te;
+    te.threads = filter == FGSS_FILTER_WARP ? 32 : 128;
+    te.hash_log2 = filter == FGSS_FILTER_WARP ? 9 : 11;
+    te.regs_rt = filter == FGSS_FILTER_WARP ? 1024 : 768;
+    te.ctas_per_sm = 0;
+    te.heavy_min_probe = filter == FGSS_FILTER_GLOBAL ? 1 : 0;
+    return te;
+}
+
+// The strategy a tuned entry amounts to.
+int filter_of(const TuneEntry& te) {
+    return te.heavy_min_probe == 1 ? FGSS_FILTER_GLOBAL : te.threads == 32 ? FGSS_FILTER_WARP : FGSS_FILTER_CTA;
+}
+
 // sided: the batch is an R-S join (its records carry a side byte)
 void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const FusedArgs* d_fargs, const uint4* items,
                   uint32_t n_items, uint32_t* counter, bool sided) {
@@ -302,6 +318,7 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
                 lead = i;
         te = c.tune_force ? *c.tune_force
                           : tune_lookup(c, tune_key(joins[lead]->in.n_sets, joins[lead]->in.n_tokens, joins[lead]->t));
+        if (!c.tune_force && joins[lead]->filter != FGSS_FILTER_AUTO) te = filter_entry(joins[lead]->filter);
     }
     const uint32_t cap_entries = (1u << te.hash_log2) / 2;  // chunk capacity of the chosen kernel shape
     for (size_t i = 0; i < nj; i++) {
@@ -395,6 +412,7 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
         }
         JoinArgs& a = J.args;
         a.res_cap = (uint32_t)cap;
+        a.heavy_min_qp = te.heavy_min_probe > 0 ? (uint32_t)te.heavy_min_probe : 0xffffffffu;
         a.res_q = c.devT<uint32_t>(J.pfx("res.q"), cap + 1);
         a.res_s = c.devT<uint32_t>(J.pfx("res.s"), cap + 1);
         a.res_o = c.devT<uint32_t>(J.pfx("res.o"), cap + 1);

@@ -26,6 +26,8 @@ struct TuneEntry {
     int hash_log2 = 9;     // shared-memory slot table (log2)
     int regs_rt = 1024;    // resident threads per SM the register budget is sized for
     int ctas_per_sm = 0;   // persistent grid = ctas_per_sm x SMs (0 = as many as fit)
+    int heavy_min_probe = 0;  // queries with a probe prefix this long take the global accumulator (0: only
+                              // those beyond the fused kernel's shared-memory caps)
     float ms = 0.f;        // best time seen
 };
 

@@ -84,6 +84,8 @@ void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_o
     J.t = o.threshold;
     J.res_cap_user = o.result_capacity;
     J.bounds = o.bounds;
+    J.filter = o.filter;
+    if (o.filter < FGSS_FILTER_AUTO || o.filter > FGSS_FILTER_GLOBAL) fail(FGSS_ERR_INVALID, "unknown filter strategy");
     if (!(o.threshold > 0.0f && o.threshold < 1.0f))
         fail(FGSS_ERR_INVALID, "threshold must be in (0, 1) (fgssjoin_cli.cu:31-35)");
     if (v.n_sets >= 0xffffffffull) fail(FGSS_ERR_UNSUPPORTED, "more than 2^32-1 records");

@@ -33,6 +33,7 @@ struct JoinState {
     const uint32_t* id = nullptr;
     float t = 0.f;
     int bounds = 0;
+    int filter = 0;            // FGSS_FILTER_* (batched method)
     DevBounds lut{};
     JoinArgs args{};
     JoinArgs* d_args = nullptr;
@@ -106,6 +107,8 @@ void join_query_costs(Ctx& c, JoinState& J, bool use_model, uint64_t* out);
 std::string tune_key(uint64_t n, uint64_t n_tokens, float t);
 extern const int kFusedShapes[][3];
 extern const int kNumFusedShapes;
+TuneEntry filter_entry(int filter);   // the launch shape of a requested FGSS_FILTER_* strategy
+int filter_of(const TuneEntry& te);   // the FGSS_FILTER_* strategy a tuned entry amounts to
 TuneEntry tune_lookup(Ctx& c, const std::string& key);
 void tune_load(Ctx& c);
 void tune_save(Ctx& c);

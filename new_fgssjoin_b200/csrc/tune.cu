@@ -1,6 +1,6 @@
 // tune.cu -- the autotuner's cache: the best launch shape of the batched
 // method's fused kernel per workload class, kept in the context and in a small
-// JSON file ({"key": [threads, hash_log2, regs_rt, ctas_per_sm, ms], ...}).
+// JSON file ({"key": [threads, hash_log2, regs_rt, ctas_per_sm, ms, heavy_min_probe], ...}).
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
@@ -37,19 +37,22 @@ void tune_load(Ctx& c) {
     char line[512];
     while (fgets(line, sizeof line, f)) {
         char key[128];
-        int th, hl, rt, cps;
+        int th, hl, rt, cps, hmp = 0;
         float ms;
-        if (sscanf(line, " \"%127[^\"]\" : [ %d , %d , %d , %d , %f ]", key, &th, &hl, &rt, &cps, &ms) == 6) {
+        const int got = sscanf(line, " \"%127[^\"]\" : [ %d , %d , %d , %d , %f , %d ]", key, &th, &hl, &rt, &cps, &ms,
+                               &hmp);
+        if (got == 6 || got == 7) {
             bool known = false;
             for (int i = 0; i < kNumFusedShapes; i++)
                 known |= kFusedShapes[i][0] == th && kFusedShapes[i][1] == hl && kFusedShapes[i][2] == rt;
-            if (!known || cps < 0 || cps > 64) continue;  // a stale or foreign entry is ignored
+            if (!known || cps < 0 || cps > 64 || hmp < 0 || hmp > 1) continue;  // a stale or foreign entry is ignored
             TuneEntry e;
             e.threads = th;
             e.hash_log2 = hl;
             e.regs_rt = rt;
             e.ctas_per_sm = cps;
             e.ms = ms;
+            e.heavy_min_probe = hmp;
             c.tune[key] = e;
         }
     }
@@ -65,8 +68,8 @@ void tune_save(Ctx& c) {
     bool first = true;
     for (auto& kv : c.tune) {
         if (kv.first.compare(0, 6, "fused.") != 0) continue;
-        fprintf(f, "%s \"%s\": [%d, %d, %d, %d, %.4f]", first ? "" : ",\n", kv.first.c_str(), kv.second.threads,
-                kv.second.hash_log2, kv.second.regs_rt, kv.second.ctas_per_sm, kv.second.ms);
+        fprintf(f, "%s \"%s\": [%d, %d, %d, %d, %.4f, %d]", first ? "" : ",\n", kv.first.c_str(), kv.second.threads,
+                kv.second.hash_log2, kv.second.regs_rt, kv.second.ctas_per_sm, kv.second.ms, kv.second.heavy_min_probe);
         first = false;
     }
     fprintf(f, "\n}\n");
