@@ -7,7 +7,9 @@
 #                compiled on the host: the float32 bound tables
 #   ref_load     oracle/ref_load.cu over its src/fgssjoin/data.cu loader
 #                (ppjoin_format, host code only): the .bin record order
-# The reference's join kernels are not run here.
+#   ref_join     oracle/ref_join.cu over its join kernels (data, index,
+#                filtering, checking, compaction, util): the reference's own
+#                GPU join with one tile, run by the GPU tests on a B200
 set -e
 REF=${FGSS_REFERENCE:-/root/reference}  # where the reference checkout lies
 HERE=$(cd "$(dirname "$0")" && pwd)
@@ -31,4 +33,12 @@ if [ "$HERE/ref_load.cu" -nt "$OUT/ref_load" ] || [ ! -x "$OUT/ref_load" ]; then
         "$HERE/ref_load.cu" "$REF/src/fgssjoin/data.cu" "$REF/src/util.cu" "$REF/src/util.cpp" "$REF/src/io.cpp" \
         -o "$OUT/ref_load" -lcuda
     echo "built $OUT/ref_load"
+fi
+if [ "$HERE/ref_join.cu" -nt "$OUT/ref_join" ] || [ ! -x "$OUT/ref_join" ]; then
+    "$NVCC" -O3 -std=c++14 -w -gencode arch=compute_100a,code=sm_100a \
+        -I"$REF/include" -I"$REF/include/fgssjoin" \
+        "$HERE/ref_join.cu" "$REF/src/fgssjoin/data.cu" "$REF/src/fgssjoin/index.cu" \
+        "$REF/src/fgssjoin/filtering.cu" "$REF/src/fgssjoin/checking.cu" "$REF/src/fgssjoin/compaction.cu" \
+        "$REF/src/util.cu" "$REF/src/util.cpp" "$REF/src/io.cpp" -o "$OUT/ref_join"
+    echo "built $OUT/ref_join"
 fi
