@@ -452,17 +452,9 @@ void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_mode
             if (!nh && !plan) slots = 0;
         }
         if (!slots) continue;
-        uint64_t words = 4 * J.in.n_sets + 65536 + 65537;
-        words = (words + 63) & ~63ull;
-        const std::string name = c.bpfx + "heavy.scratch";
-        auto it = c.bufs.find(name);
-        const size_t need = words * slots * 4;
-        const bool grow = it == c.bufs.end() || it->second.bytes < need;
-        if (grow && capture) fail(FGSS_ERR_CUDA, "heavy scratch would grow inside a graph capture");
-        uint32_t* scratch = (uint32_t*)c.dev(name, need);
-        if (grow) FGSS_CK(cudaMemsetAsync(scratch, 0, c.bufs[name].bytes, c.stream));
-        k_probe_heavy<MODE_FUSED, 512><<<slots, 512, 0, c.stream>>>(d_args, (uint32_t)i, scratch, words,
-                                                                    counter + 4 + i);
+        const HeavyScratch hs = heavy_scratch(c, c.bpfx, J.in.n_sets, slots, capture);
+        k_probe_heavy<MODE_FUSED, 512><<<slots, 512, 0, c.stream>>>(d_args, (uint32_t)i, hs.zero, hs.zero_words, hs.aux,
+                                                                    hs.aux_words, counter + 4 + i);
         FGSS_LAUNCH_CK();
     }
     if (plan && !capture) {

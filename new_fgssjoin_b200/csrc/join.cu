@@ -220,19 +220,19 @@ void join_finish_status(Ctx& c, JoinState& J) {
         fail(FGSS_ERR_CUDA, "internal table overflow in the filter (status " + std::to_string(J.status_host) + ")");
 }
 
-// Heavy-path scratch for `slots` CTAs of a join of n records (zeroed once;
-// the kernel leaves it zero after every query).
-static uint32_t* heavy_scratch(Ctx& c, uint64_t n, uint32_t slots, uint64_t* slot_words) {
-    uint64_t w = 4 * n + 65536 + 65537;
-    w = (w + 63) & ~63ull;
-    *slot_words = w;
-    const std::string name = "heavy.scratch";
-    auto it = c.bufs.find(name);
-    size_t need = w * slots * 4;
-    bool grow = it == c.bufs.end() || it->second.bytes < need;
-    uint32_t* p = (uint32_t*)c.dev(name, need);
-    if (grow) FGSS_CK(cudaMemsetAsync(p, 0, c.bufs[name].bytes, c.stream));
-    return p;
+HeavyScratch heavy_scratch(Ctx& c, const std::string& prefix, uint64_t n, uint32_t slots, bool capture) {
+    HeavyScratch h;
+    h.zero_words = (2 * n + 63) & ~63ull;
+    h.aux_words = (2 * n + 65536 + 65537 + 63) & ~63ull;
+    const std::string zn = prefix + "heavy.zero";
+    auto it = c.bufs.find(zn);
+    const size_t need = h.zero_words * slots * 4;
+    const bool grow = it == c.bufs.end() || it->second.bytes < need;
+    if (grow && capture) fail(FGSS_ERR_CUDA, "heavy scratch would grow inside a graph capture");
+    h.zero = (uint32_t*)c.dev(zn, need);
+    if (grow) FGSS_CK(cudaMemsetAsync(h.zero, 0, c.bufs[zn].bytes, c.stream));
+    h.aux = c.devT<uint32_t>(prefix + "heavy.aux", h.aux_words * slots);
+    return h;
 }
 
 void join_plain_filter_verify(Ctx& c, JoinState& J, bool want_cand) {
@@ -265,13 +265,13 @@ void join_plain_filter_verify(Ctx& c, JoinState& J, bool want_cand) {
     FGSS_CK(cudaMemcpyAsync(hcnt, a.heavy_count, 4, cudaMemcpyDeviceToHost, c.stream));
     c.sync();
     const uint32_t nheavy = hcnt[0];
-    uint64_t slot_words = 0;
-    uint32_t* scratch = nullptr;
+    HeavyScratch hs;
     uint32_t hslots = std::min<uint32_t>(nheavy, (uint32_t)c.num_sms);
     if (nheavy) {
-        scratch = heavy_scratch(c, n, hslots, &slot_words);
+        hs = heavy_scratch(c, "", n, hslots, false);
         FGSS_CK(cudaMemsetAsync(qctr, 0, 4, c.stream));
-        k_probe_heavy<MODE_COUNT, 512><<<hslots, 512, 0, c.stream>>>(J.d_args, 0, scratch, slot_words, qctr);
+        k_probe_heavy<MODE_COUNT, 512><<<hslots, 512, 0, c.stream>>>(J.d_args, 0, hs.zero, hs.zero_words, hs.aux,
+                                                                     hs.aux_words, qctr);
         FGSS_LAUNCH_CK();
     }
     exclusive_scan<uint32_t>(c, a.vcnt, voff, n, nullptr, tot, J.pfx("scan.v").c_str());
@@ -294,7 +294,8 @@ void join_plain_filter_verify(Ctx& c, JoinState& J, bool want_cand) {
     FGSS_LAUNCH_CK();
     if (nheavy) {
         FGSS_CK(cudaMemsetAsync(qctr, 0, 4, c.stream));
-        k_probe_heavy<MODE_FILL, 512><<<hslots, 512, 0, c.stream>>>(J.d_args, 0, scratch, slot_words, qctr);
+        k_probe_heavy<MODE_FILL, 512><<<hslots, 512, 0, c.stream>>>(J.d_args, 0, hs.zero, hs.zero_words, hs.aux,
+                                                                    hs.aux_words, qctr);
         FGSS_LAUNCH_CK();
     }
     uint64_t* d_nc = c.devT<uint64_t>(J.pfx("nc"), 2);

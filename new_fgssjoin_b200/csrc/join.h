@@ -88,6 +88,16 @@ void join_features(Ctx& c, JoinState& J, float* d_feat);
 void join_finish_status(Ctx& c, JoinState& J);  // D2H of status + stats, throws on bad input
 void join_output(Ctx& c, JoinState& J, uint64_t* keys, uint32_t* vals, const uint64_t* d_n, uint64_t n_cap);
 
+// Scratch of the global-memory accumulator kernel (k_probe_heavy) for `slots`
+// CTAs of a join of n records, in the buffer namespace `prefix`: the always-zero
+// per-source counters (zeroed when allocated) and the other per-query arrays.
+struct HeavyScratch {
+    uint32_t* zero = nullptr;
+    uint32_t* aux = nullptr;
+    uint64_t zero_words = 0, aux_words = 0;
+};
+HeavyScratch heavy_scratch(Ctx& c, const std::string& prefix, uint64_t n, uint32_t slots, bool capture);
+
 // Host-side decisions of one batched run, recorded eagerly and reused when the
 // same batch is captured into a CUDA graph (batch.cu).
 struct BatchPlan {

@@ -705,18 +705,24 @@ __global__ void __launch_bounds__(NT) k_probe(const JoinArgs* __restrict__ joins
 // Queries past the shared-memory caps (long records): a per-CTA dense
 // accumulator in global memory, slot = source id.  The entries' source
 // positions give the exact last match directly.
+// Scratch per CTA slot: `zero` holds the per-source counters gcnt, gmp (n
+// words each), all zero between queries (zeroed once when allocated; every
+// query clears the sources it touched), in a buffer of their own so that no
+// other array, whatever its layout for another join, ever dirties them;
+// `aux` holds the touched and verify lists and the query's windows.
 template <int MODE, int NT>
 __global__ void __launch_bounds__(NT) k_probe_heavy(const JoinArgs* __restrict__ joins, uint32_t join_id,
-                                                    uint32_t* __restrict__ scratch, uint64_t slot_words,
+                                                    uint32_t* __restrict__ zero, uint64_t zero_words,
+                                                    uint32_t* __restrict__ aux, uint64_t aux_words,
                                                     uint32_t* queue_counter) {
     const JoinArgs& a = joins[join_id];
     const uint32_t n = a.n;
-    uint32_t* base = scratch + (uint64_t)blockIdx.x * slot_words;
-    uint32_t* gcnt = base;
-    uint32_t* gmp = base + n;
-    uint32_t* gtouch = base + 2 * (uint64_t)n;
-    uint32_t* gver = base + 3 * (uint64_t)n;
-    uint32_t* wlo = base + 4 * (uint64_t)n;
+    uint32_t* gcnt = zero + (uint64_t)blockIdx.x * zero_words;
+    uint32_t* gmp = gcnt + n;
+    uint32_t* base = aux + (uint64_t)blockIdx.x * aux_words;
+    uint32_t* gtouch = base;
+    uint32_t* gver = base + (uint64_t)n;
+    uint32_t* wlo = base + 2 * (uint64_t)n;
     uint32_t* wpre = wlo + 65536;
     __shared__ uint32_t s_item, s_nt, s_nv, s_tot, s_nc;
     __shared__ uint32_t wsum[33];

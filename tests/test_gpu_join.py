@@ -256,6 +256,18 @@ def test_filter_strategies_match_oracle(ctx, titles_sets, filt, t):
         assert got.stats["heavy_queries"] > 0
 
 
+def test_global_accumulator_joins_of_different_sizes_in_turn():
+    """The global-memory accumulator's per-source counters must be zero when a
+    query starts, whatever join of whatever size used the scratch before: joins
+    of 9,000, then 2,500, then 6,000 records in one context, each against the oracle."""
+    with F.Context(device=0) as c2:
+        for n, seed, t in ((9000, 41, 0.6), (2500, 42, 0.5), (6000, 43, 0.7)):
+            s = c2.tokenize(datagen.titles(n, seed=seed), **datagen.TITLE_TOK)
+            ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, t)
+            for method, filt in (("batched", "global"), ("plain", "auto")):
+                _check_same(c2.selfjoin(s, t, method=method, filter=filt), ref, st)
+
+
 @pytest.mark.parametrize("filt", ["warp", "global"])
 def test_filter_strategies_on_heavy_tailed_records(ctx, filt):
     s = ctx.tokenize(datagen.heavy(4000, seed=19), **datagen.TITLE_TOK)
