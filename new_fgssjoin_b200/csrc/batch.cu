@@ -121,6 +121,7 @@ int fused_resident_ctas(Ctx& c, const TuneEntry& te) {
     FGSS_R(128, 10, 768)
     FGSS_R(128, 11, 768)
     FGSS_R(256, 11, 768)
+    FGSS_R(256, 12, 768)
 #undef FGSS_R
     return resident_ctas<64, 9, 768>(c);
 }
@@ -148,8 +149,8 @@ static void launch_fused(Ctx& c, const JoinArgs* d_args, const FusedArgs* d_farg
 // resident threads per SM the register budget is sized for.
 extern const int kFusedShapes[][3] = {{32, 8, 1024},  {32, 9, 1024},  {64, 9, 1024},   {64, 9, 768},
                                       {64, 10, 1024}, {128, 9, 1024}, {128, 10, 1024}, {128, 10, 768},
-                                      {128, 11, 768}, {256, 11, 768}};
-extern const int kNumFusedShapes = 10;
+                                      {128, 11, 768}, {256, 11, 768},  {256, 12, 768}};
+extern const int kNumFusedShapes = 11;
 
 // The launch shape that stands for a requested filter strategy.
 TuneEntry filter_entry(int filter) {
@@ -186,6 +187,7 @@ void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const Fus
     FGSS_F(128, 10, 768)
     FGSS_F(128, 11, 768)
     FGSS_F(256, 11, 768)
+    FGSS_F(256, 12, 768)
 #undef FGSS_F
     if (sided) launch_fused<64, 9, 768, true>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm);
     else launch_fused<64, 9, 768, false>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm);

@@ -28,7 +28,7 @@ namespace fgss {
 // number of prefix matches (10).
 constexpr uint32_t kSmaxUnknown = 2047;
 
-// Layout: slots u64[H] | occ u16[H] | sls u16[H] | chk u16[H/2] | wlo,whi,clo u32[PC] |
+// Layout: slots u64[H] | occ u16[H] | sls u16[H] | wlo,whi,clo u32[PC] |
 //         wpre u32[PC+4] | qtok u32[QC] | bm u32[BW] | mlist u16[MC]
 template <int HLOG>
 struct FusedLayout {
@@ -37,13 +37,13 @@ struct FusedLayout {
     // probe tokens handled in shared memory: 256..512 (a slot's 11-bit query
     // position and 10-bit match count rely on PC <= 512)
     static constexpr uint32_t PC = H / 4 > 512 ? 512 : (H / 4 > 256 ? H / 4 : 256);
-    static constexpr uint32_t QC = H / 2;     // query tokens staged in shared memory (longer: read from HBM)
+    static constexpr uint32_t QC = H / 2 > 1024 ? 1024 : H / 2;  // query tokens staged in shared memory
+                                                                  // (longer: read from HBM)
     static constexpr uint32_t BW = 1024;      // bitmap words: 32768 bits
     static constexpr uint32_t MC = 512;       // merge list entries per chunk (more: merged by their lane)
     static constexpr size_t off_occ = 8ull * H;
     static constexpr size_t off_sls = off_occ + 2ull * H;   // source size of each slot
-    static constexpr size_t off_chk = off_sls + 2ull * H;   // bitmap-check list (<= one per occupied slot <= cap)
-    static constexpr size_t off_wlo = off_chk + 1ull * H;
+    static constexpr size_t off_wlo = off_sls + 2ull * H;
     static constexpr size_t off_whi = off_wlo + 4ull * PC;
     static constexpr size_t off_clo = off_whi + 4ull * PC;
     static constexpr size_t off_wpre = off_clo + 4ull * PC;
@@ -271,13 +271,11 @@ __device__ __forceinline__ void tally_overlap(const JoinArgs& a, FusedCounters& 
 //      with one 64-bit CAS (key s; match count, last match positions); a
 //      newly occupied slot records the source's size beside it and is appended
 //      to the occupied list (one shared atomic per warp);
-//   2a. decide from shared memory: per occupied slot the reference-candidate
-//      and needs-merge tests read the slot word, the size beside it and the
-//      bound table (no gather per source); slots that need a merge go on the
-//      bitmap-check list;
-//   2b. bitmap bound: bmw lanes per listed source, one 16-byte word each (a
-//      warp loads 8 or 16 bitmaps with one instruction); sources whose bound
-//      can still reach floor(min overlap) go on the merge list;
+//   2. decide: per occupied slot the reference-candidate and needs-merge tests
+//      read the slot word, the size beside it and the bound table (no gather
+//      per source); a slot that still needs a merge loads the source's bitmap
+//      (2 or 4 16-byte words) and, if the bitmap bound can still reach
+//      floor(min overlap), goes on the merge list (one shared atomic per warp);
 //   3. merge: warps take the merge list, 32 source tokens per step (one
 //      coalesced load, a membership test per lane, ballot + popcount), with
 //      the early exit of checking.cu:150-157; slots are cleared meanwhile.
@@ -290,7 +288,6 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem);
     uint16_t* occ = reinterpret_cast<uint16_t*>(smem + Lay::off_occ);
     uint16_t* sls = reinterpret_cast<uint16_t*>(smem + Lay::off_sls);
-    uint16_t* chk = reinterpret_cast<uint16_t*>(smem + Lay::off_chk);
     uint32_t* wlo = reinterpret_cast<uint32_t*>(smem + Lay::off_wlo);
     uint32_t* whi = reinterpret_cast<uint32_t*>(smem + Lay::off_whi);
     uint32_t* clo = reinterpret_cast<uint32_t*>(smem + Lay::off_clo);
@@ -298,10 +295,10 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     uint32_t* qtok = reinterpret_cast<uint32_t*>(smem + Lay::off_qtok);
     uint32_t* bm = reinterpret_cast<uint32_t*>(smem + Lay::off_bm);
     uint16_t* mlist = reinterpret_cast<uint16_t*>(smem + Lay::off_ml);
-    __shared__ uint32_t s_sp, s_nocc, s_nchk, s_nm, s_cand, s_win;
+    __shared__ uint32_t s_sp, s_nocc, s_nm, s_cand, s_win, s_L;
     __shared__ uint4 s_qbm[4];  // the query's bitmap
     __shared__ uint32_t s_sa[48], s_sb[48], s_sc[48];
-    __shared__ uint32_t wsum[33];
+    constexpr uint32_t kNoPart = 0xffffffffu, kBisected = 0xfffffffeu;  // s_L: no part left / bisected
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const uint32_t st_bits = *a.status;
@@ -353,7 +350,6 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
         s_win = 0;
         s_sp = 0;
         s_nocc = 0;
-        s_nchk = 0;
         s_nm = 0;
         ctr.qtok += lq;
         if (one_chunk) wpre[qp] = qm.w;
@@ -384,70 +380,67 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                 L = qm.w;
                 if (tid == 0) s_win += L;
             } else {
-                __syncthreads();
-                const uint32_t sp = s_sp;
-                if (sp == 0) break;
-                const uint32_t ra = s_sa[sp - 1], rb = s_sb[sp - 1], tag = s_sc[sp - 1];
-                constexpr uint32_t PER = (Lay::PC + NT - 1) / NT;
-                const uint32_t b0 = tid * PER;
-                uint32_t loc[PER];
-                uint32_t sum = 0;
-#pragma unroll
-                for (uint32_t i = 0; i < PER; i++) {
-                    const uint32_t j = b0 + i;
-                    uint32_t cnt = 0;
-                    if (j < qp) {
-                        uint32_t lo, hi;
-                        if (tag != 0xffffffffu) {
-                            lo = tag == 0 ? wlo[j] : cb[(tag - 1) * qp + j];
-                            hi = tag + 1 == nch ? whi[j] : cb[tag * qp + j];
-                        } else {
-                            lo = lower_bound_u32(a.ent_s, wlo[j], whi[j], ra);
-                            hi = lower_bound_u32(a.ent_s, lo, whi[j], rb);
+                __syncthreads();  // the previous part is done with the slots and the windows
+                if (wid == 0) {
+                    // warp 0: this part's windows and their exclusive prefix, and whether
+                    // it must be bisected further (then its halves go on the stack)
+                    const uint32_t sp = s_sp;
+                    const uint32_t ra = sp ? s_sa[sp - 1] : 0, rb = sp ? s_sb[sp - 1] : 0;
+                    const uint32_t tag = sp ? s_sc[sp - 1] : 0;
+                    __syncwarp();
+                    if (sp == 0) {
+                        if (lane == 0) s_L = kNoPart;
+                    } else {
+                        uint32_t carry = 0;
+                        for (uint32_t j0 = 0; j0 < qp; j0 += 32) {
+                            const uint32_t j = j0 + lane;
+                            uint32_t cnt = 0;
+                            if (j < qp) {
+                                uint32_t lo, hi;
+                                if (tag != 0xffffffffu) {
+                                    lo = tag == 0 ? wlo[j] : cb[(tag - 1) * qp + j];
+                                    hi = tag + 1 == nch ? whi[j] : cb[tag * qp + j];
+                                } else {
+                                    lo = lower_bound_u32(a.ent_s, wlo[j], whi[j], ra);
+                                    hi = lower_bound_u32(a.ent_s, lo, whi[j], rb);
+                                }
+                                cnt = hi - lo;
+                                clo[j] = lo;
+                            }
+                            const uint32_t incl = warp_incl_scan(cnt);
+                            if (j < qp) wpre[j] = carry + incl - cnt;
+                            carry += __shfl_sync(kFull, incl, 31);
                         }
-                        cnt = hi - lo;
-                        clo[j] = lo;
+                        if (lane == 0) {
+                            if (carry > Lay::cap && rb - ra > 1) {  // bisect; the lower half first
+                                const uint32_t mid = ra + (rb - ra) / 2;
+                                s_sa[sp - 1] = mid;
+                                s_sb[sp - 1] = rb;
+                                s_sc[sp - 1] = 0xffffffffu;
+                                s_sa[sp] = ra;
+                                s_sb[sp] = mid;
+                                s_sc[sp] = 0xffffffffu;
+                                s_sp = sp + 1;
+                                s_L = kBisected;
+                            } else {
+                                wpre[qp] = carry;
+                                s_sp = sp - 1;
+                                s_win += carry;
+                                s_L = carry;
+                            }
+                        }
                     }
-                    loc[i] = cnt;
-                    sum += cnt;
                 }
-                // (its barriers also order every thread's read of the stack top
-                // before thread 0 changes it below)
-                uint32_t pre = block_excl_scan<uint32_t>(sum, wsum, &L);
-#pragma unroll
-                for (uint32_t i = 0; i < PER; i++) {
-                    const uint32_t j = b0 + i;
-                    if (j < qp) wpre[j] = pre;
-                    pre += loc[i];
-                }
-                if (L > Lay::cap && rb - ra > 1) {
-                    if (tid == 0) {  // bisect an oversized range; the lower half first
-                        const uint32_t mid = ra + (rb - ra) / 2;
-                        s_sa[sp - 1] = mid;
-                        s_sb[sp - 1] = rb;
-                        s_sc[sp - 1] = 0xffffffffu;
-                        s_sa[sp] = ra;
-                        s_sb[sp] = mid;
-                        s_sc[sp] = 0xffffffffu;
-                        s_sp = sp + 1;
-                    }
-                    continue;
-                }
-                if (tid == 0) {
-                    wpre[qp] = L;
-                    s_sp = sp - 1;
-                    s_win += L;
-                }
-                if (L == 0) continue;
-                __syncthreads();  // wpre complete
+                __syncthreads();  // the part's windows, prefix and fate
+                L = s_L;
+                if (L == kNoPart) break;
+                if (L == kBisected) continue;
             }
             if (L == 0) continue;
             int hl = 6;
             while ((1u << hl) < 2 * L && hl < HLOG) hl++;
             const uint32_t mask = (1u << hl) - 1;
-            // 1. accumulate.  A lane's entries f increase, so its token index j
-            // only moves forward; four entries' loads are issued before their
-            // slot updates.
+            // 1. accumulate: four entries' loads are issued before their slot updates.
             uint32_t j = 0;
             for (uint32_t f0 = tid - lane; f0 < L; f0 += 4 * NT) {
                 uint32_t sv[4], pv[4], jv[4];
@@ -456,7 +449,16 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                     const uint32_t f = f0 + lane + u * NT;
                     sv[u] = kEmpty;
                     if (f < L) {
-                        while (wpre[j + 1] <= f) j++;
+                        {   // the window holding entry f: the last j with wpre[j] <= f (a
+                            // binary search: its trip count is the same on every lane)
+                            uint32_t lo2 = 0, hi2 = qp;
+                            while (lo2 < hi2) {
+                                const uint32_t mid = (lo2 + hi2) >> 1;
+                                if (wpre[mid] <= f) lo2 = mid + 1;
+                                else hi2 = mid;
+                            }
+                            j = lo2 - 1;
+                        }
                         const uint32_t k = clo[j] + (f - wpre[j]);
                         sv[u] = __ldg(a.ent_s + k);
                         pv[u] = __ldg(a.ent_pl + k);  // source size << 16 | source position
@@ -518,7 +520,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                 }
             }
             __syncthreads();
-            // 2a. decide from shared memory: reference candidate?  needs a merge?
+            // 2. decide: reference candidate?  needs a merge?  (bitmap bound last)
             const uint32_t nocc = s_nocc;
             uint32_t my_cand = 0;
             for (uint32_t i0 = tid - lane; i0 < nocc; i0 += NT) {
@@ -551,72 +553,47 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                         // the merge resumes right after the last match (or at c when its position
                         // was not kept); when nothing left can change the count, c is the overlap
                         const uint32_t k = smx != kSmaxUnknown ? smx + 1 : c;
-                        if (k >= ls || c + min(ls - k, A - 1) < sm.y) tally_overlap(a, ctr, q, s, c, sm.y, sm.z);
-                        else check = true;
+                        if (k >= ls || c + min(ls - k, A - 1) < sm.y) {
+                            tally_overlap(a, ctr, q, s, c, sm.y, sm.z);
+                        } else {
+                            // bitmap bound on the whole overlap: below floor(min overlap), no merge
+                            const uint4* b4 = fa.bmap + fa.bmw * s;
+                            uint32_t pc = popc_xor(s_qbm[0], __ldg(b4)) + popc_xor(s_qbm[1], __ldg(b4 + 1));
+                            if (fa.bmw == 4) pc += popc_xor(s_qbm[2], __ldg(b4 + 2)) + popc_xor(s_qbm[3], __ldg(b4 + 3));
+                            check = lq + ls >= 2 * sm.y + pc;
+                        }
                     }
                 }
                 const uint32_t m = __ballot_sync(kFull, check);
-                if (m) {  // onto the bitmap-check list, one shared atomic per warp
+                if (m) {  // onto the merge list
                     uint32_t base = 0;
-                    if (lane == 0) base = atomicAdd(&s_nchk, (uint32_t)__popc(m));
+                    if (lane == 0) base = atomicAdd(&s_nm, (uint32_t)__popc(m));
                     base = __shfl_sync(kFull, base, 0);
-                    if (check) chk[base + __popc(m & lanemask_lt())] = (uint16_t)h;
-                }
-            }
-            my_cand = warp_sum(my_cand);
-            if (lane == 0 && my_cand) atomicAdd(&s_cand, my_cand);
-            __syncthreads();
-            // 2b. bitmap bound on the whole overlap, bmw lanes per listed source (one
-            // 16-byte word each: a warp loads 32 / bmw bitmaps with one instruction);
-            // a bound below floor(min overlap) means no merge can reach it
-            {
-                const uint32_t nchk = s_nchk, bmw = fa.bmw, G = 32u / bmw;
-                const uint32_t part = lane & (bmw - 1u), grp = lane / bmw;
-                const uint4 qw = s_qbm[part];
-                for (uint32_t e0 = wid * G; e0 < nchk; e0 += NW * G) {
-                    const uint32_t e = e0 + grp;
-                    uint32_t h = 0, pc = 0;
-                    if (e < nchk) {
-                        h = chk[e];
-                        const uint32_t s = (uint32_t)(slots[h] >> 32);
-                        pc = popc_xor(qw, __ldg(fa.bmap + bmw * s + part));
-                    }
-                    pc += __shfl_xor_sync(kFull, pc, 1);
-                    if (bmw == 4) pc += __shfl_xor_sync(kFull, pc, 2);
-                    bool merge = false;
-                    if (e < nchk && part == 0) {
-                        const uint32_t ls = sls[h];
-                        merge = lq + ls >= 2 * __ldg(smin + ls).y + pc;
-                    }
-                    const uint32_t m = __ballot_sync(kFull, merge);
-                    if (m) {  // onto the merge list
-                        uint32_t base = 0;
-                        if (lane == 0) base = atomicAdd(&s_nm, (uint32_t)__popc(m));
-                        base = __shfl_sync(kFull, base, 0);
-                        if (merge) {
-                            const uint32_t mi = base + __popc(m & lanemask_lt());
-                            if (mi < Lay::MC) {
-                                mlist[mi] = (uint16_t)h;
-                            } else {
-                                // the merge list is full: this lane merges the source itself
-                                const unsigned long long v = slots[h];
-                                const uint32_t s = (uint32_t)(v >> 32), lo = (uint32_t)v;
-                                const uint32_t c = lo & 0x3ffu, jm = lo >> 21, smx = (lo >> 10) & 0x7ffu;
-                                const uint32_t ls = sls[h];
-                                const uint4 sm = __ldg(smin + ls);
-                                const uint32_t* st = a.tok + fa.meta[s].x;
-                                const uint32_t xq = qsrc[jm], qrest = lq - jm - 1;
-                                const uint32_t k0 = smx != kSmaxUnknown ? smx + 1 : c;
-                                uint32_t k = k0, cnt = c;
-                                while (k < ls && cnt + min(ls - k, qrest - (cnt - c)) >= sm.y)
-                                    cnt += merge_step(st, k, ls, xq, bm, qmode, qsrc, lq);
-                                ctr.merged += k - k0;
-                                tally_overlap(a, ctr, q, s, cnt, sm.y, sm.z);
-                            }
+                    if (check) {
+                        const uint32_t mi = base + __popc(m & lanemask_lt());
+                        if (mi < Lay::MC) {
+                            mlist[mi] = (uint16_t)h;
+                        } else {
+                            // the merge list is full: this lane merges the source itself
+                            const unsigned long long v = slots[h];
+                            const uint32_t s = (uint32_t)(v >> 32), lo = (uint32_t)v;
+                            const uint32_t c = lo & 0x3ffu, jm = lo >> 21, smx = (lo >> 10) & 0x7ffu;
+                            const uint32_t ls = sls[h];
+                            const uint4 sm = __ldg(smin + ls);
+                            const uint32_t* st = a.tok + fa.meta[s].x;
+                            const uint32_t xq = qsrc[jm], qrest = lq - jm - 1;
+                            const uint32_t k0 = smx != kSmaxUnknown ? smx + 1 : c;
+                            uint32_t k = k0, cnt = c;
+                            while (k < ls && cnt + min(ls - k, qrest - (cnt - c)) >= sm.y)
+                                cnt += merge_step(st, k, ls, xq, bm, qmode, qsrc, lq);
+                            ctr.merged += k - k0;
+                            tally_overlap(a, ctr, q, s, cnt, sm.y, sm.z);
                         }
                     }
                 }
             }
+            my_cand = warp_sum(my_cand);
+            if (lane == 0 && my_cand) atomicAdd(&s_cand, my_cand);
             __syncthreads();
             // 3. merge the listed sources (a warp per source) and clear the slots
             const uint32_t nm = min(s_nm, Lay::MC);
@@ -648,13 +625,13 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                 }
             }
             __syncthreads();  // the merges read the slots
+            // (the next barrier -- the next part's first, or the query's last -- orders
+            // this clear before any later accumulate)
             for (uint32_t i2 = tid; i2 < nocc; i2 += NT) slots[occ[i2]] = kEmptySlot;
             if (tid == 0) {
                 s_nocc = 0;
-                s_nchk = 0;
                 s_nm = 0;
             }
-            __syncthreads();
         }
     }
     __syncthreads();
