@@ -655,7 +655,9 @@ def main():
                for ti in (range(len(sets)) if w["kind"] == "rs" else {jobs[k][0] for k in sample})}
         v, ms, threads, note, opairs = cpu_reference(w, jobs, mem, 1, 0, keep_pairs=True)
         cpu = {"value": v, "unit": "candidates/s", "cores": threads, "kind": "port", "sample": note}
-        eq = all(np.array_equal(bat_out[k].q, p["q"]) and np.array_equal(bat_out[k].s, p["s"]) and
+        # R-S pairs carry (r, s): the GPU result's q column is the index in R
+        eq = all(np.array_equal(bat_out[k].q, p["r" if w["kind"] == "rs" else "q"]) and
+                 np.array_equal(bat_out[k].s, p["s"]) and
                  np.array_equal(bat_out[k].overlap, p["overlap"]) and np.array_equal(bat_out[k].sim, p["sim"])
                  for k, p in opairs.items())
         oracle_eq = {"equal": bool(eq), "joins_compared": len(opairs), "joins": len(jobs),

@@ -72,6 +72,19 @@ void fill_stats(const JoinState& J, fgss_stats* st) {
     st->predicted_results = J.pred_results;
 }
 
+// Host columns of R pairs (freed by fgss_pairs_free).
+void alloc_host_pairs(fgss_pairs* out, uint64_t R) {
+    const size_t b = (R ? R : 1) * 4;
+    out->q = (uint32_t*)malloc(b);
+    out->s = (uint32_t*)malloc(b);
+    out->id_q = (uint32_t*)malloc(b);
+    out->id_s = (uint32_t*)malloc(b);
+    out->overlap = (uint32_t*)malloc(b);
+    out->sim = (float*)malloc(b);
+    if (!out->q || !out->s || !out->id_q || !out->id_s || !out->overlap || !out->sim)
+        fail(FGSS_ERR_NOMEM, "host allocation for pairs");
+}
+
 void export_pairs(Ctx& c, JoinState& J, const fgss_join_opts& o, fgss_pairs* out) {
     memset(out, 0, sizeof *out);
     const uint64_t R = J.n_res;
@@ -92,15 +105,7 @@ void export_pairs(Ctx& c, JoinState& J, const fgss_join_opts& o, fgss_pairs* out
         out->sim = (float*)dup(J.osim, R * 4);
         out->on_device = 1;
     } else {
-        const size_t b = (R ? R : 1) * 4;
-        out->q = (uint32_t*)malloc(b);
-        out->s = (uint32_t*)malloc(b);
-        out->id_q = (uint32_t*)malloc(b);
-        out->id_s = (uint32_t*)malloc(b);
-        out->overlap = (uint32_t*)malloc(b);
-        out->sim = (float*)malloc(b);
-        if (!out->q || !out->s || !out->id_q || !out->id_s || !out->overlap || !out->sim)
-            fail(FGSS_ERR_NOMEM, "host allocation for pairs");
+        alloc_host_pairs(out, R);
         if (R) {
             FGSS_CK(cudaMemcpyAsync(out->q, J.oq, R * 4, cudaMemcpyDeviceToHost, c.stream));
             FGSS_CK(cudaMemcpyAsync(out->s, J.os, R * 4, cudaMemcpyDeviceToHost, c.stream));
@@ -119,36 +124,82 @@ void export_pairs(Ctx& c, JoinState& J, const fgss_join_opts& o, fgss_pairs* out
     c.sync();
 }
 
-void report_stats(Ctx& c, std::vector<JoinState*>& js, fgss_stats* stats, unsigned long long launches, int n) {
+// Pairs of every join of a batch: host outputs through one pinned staging
+// copy per column of the batch's output range, then a host copy per join.
+void export_batch(Ctx& c, Batch& B, const fgss_join_opts* opts, fgss_pairs* outs) {
+    const size_t nj = B.js.size();
+    bool staged = nj > 1;
+    for (size_t j = 0; j < nj; j++) staged &= !opts[j].out_on_device && !opts[j].want_candidates;
+    if (!staged) {
+        for (size_t j = 0; j < nj; j++) export_pairs(c, *B.js[j], opts[j], &outs[j]);
+        return;
+    }
+    const uint64_t oc = B.out_cap;
+    uint32_t* st = c.pinnedT<uint32_t>("b.stage", 6 * oc + 1);
+    const void* cols[6] = {B.oq, B.os, B.oidq, B.oids, B.oo, B.osim};
+    if (oc) {
+        for (int k = 0; k < 6; k++)
+            FGSS_CK(cudaMemcpyAsync(st + k * oc, cols[k], oc * 4, cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+    }
+    for (size_t j = 0; j < nj; j++) {
+        fgss_pairs* out = &outs[j];
+        memset(out, 0, sizeof *out);
+        const uint64_t R = B.js[j]->n_res, o = B.out_off[j];
+        out->n = R;
+        alloc_host_pairs(out, R);
+        void* dst[6] = {out->q, out->s, out->id_q, out->id_s, out->overlap, out->sim};
+        for (int k = 0; k < 6; k++) memcpy(dst[k], st + k * oc + o, R * 4);
+    }
+}
+
+// Device times of a call: index build, filter+verify, output, fused launch.
+struct Times {
+    float idx = 0, fv = 0, out = 0, probe = 0;
+};
+
+// Adds the times the events ev[0..2] (and ev[4..5]) bracket, up to now.
+void add_times(Ctx& c, Times& t) {
     cudaEvent_t* ev = c.ev;
     FGSS_CK(cudaEventRecord(ev[3], c.stream));
     FGSS_CK(cudaEventSynchronize(ev[3]));
-    float t_idx = 0, t_fv = 0, t_out = 0;
-    FGSS_CK(cudaEventElapsedTime(&t_idx, ev[0], ev[1]));
-    FGSS_CK(cudaEventElapsedTime(&t_fv, ev[1], ev[2]));
-    FGSS_CK(cudaEventElapsedTime(&t_out, ev[2], ev[3]));
-    float t_probe = 0;
-    if (c.probe_timed) FGSS_CK(cudaEventElapsedTime(&t_probe, ev[4], ev[5]));
+    float a = 0, b = 0, d = 0, e = 0;
+    FGSS_CK(cudaEventElapsedTime(&a, ev[0], ev[1]));
+    FGSS_CK(cudaEventElapsedTime(&b, ev[1], ev[2]));
+    FGSS_CK(cudaEventElapsedTime(&d, ev[2], ev[3]));
+    if (c.probe_timed) FGSS_CK(cudaEventElapsedTime(&e, ev[4], ev[5]));
+    t.idx += a;
+    t.fv += b;
+    t.out += d;
+    t.probe += e;
+}
+
+void report_stats(Ctx& c, std::vector<JoinState*>& js, fgss_stats* stats, unsigned long long launches, int n,
+                  const Times& t) {
     if (stats) {
         uint64_t* he = c.pinnedT<uint64_t>("h.E", (size_t)n + 1);
-        for (int i = 0; i < n; i++)
+        bool any = false;
+        for (int i = 0; i < n; i++) {
+            if (js[i]->n_entries != ~0ull) continue;
             FGSS_CK(cudaMemcpyAsync(he + i, js[i]->d_e, 8, cudaMemcpyDeviceToHost, c.stream));
-        c.sync();
+            any = true;
+        }
+        if (any) c.sync();
         for (int i = 0; i < n; i++) {
             memset(&stats[i], 0, sizeof(fgss_stats));
             fill_stats(*js[i], &stats[i]);
-            stats[i].index_entries = he[i];
-            stats[i].ms_index = t_idx;
-            stats[i].ms_filter = t_fv;
-            stats[i].ms_output = t_out;
-            stats[i].ms_total = t_idx + t_fv + t_out;
-            stats[i].ms_probe = t_probe;
+            stats[i].index_entries = js[i]->n_entries != ~0ull ? js[i]->n_entries : he[i];
+            stats[i].ms_index = t.idx;
+            stats[i].ms_filter = t.fv;
+            stats[i].ms_output = t.out;
+            stats[i].ms_total = t.idx + t.fv + t.out;
+            stats[i].ms_probe = t.probe;
             stats[i].launches = launches;
         }
     }
     if (c.verbose)
-        fprintf(stderr, "[fgss] joins=%d index %.3f ms, filter+verify %.3f ms, output %.3f ms\n", n, t_idx, t_fv,
-                t_out);
+        fprintf(stderr, "[fgss] joins=%d index %.3f ms, filter+verify %.3f ms, output %.3f ms\n", n, t.idx, t.fv,
+                t.out);
 }
 
 }  // namespace
@@ -167,6 +218,8 @@ struct GraphEntry {
     int failed_captures = 0;
     std::string ns;
     std::vector<std::unique_ptr<JoinState>> joins;
+    std::unique_ptr<Batch> batch;     // the batch the graph was captured from (its buffers)
+    BatchPlan plan;
     unsigned long long launches = 0;  // kernels inside the graph
     uint64_t stamp = 0;
 };
@@ -216,46 +269,68 @@ std::string graph_key(const fgss_sets_view* sets, const fgss_join_opts* opts, in
     return k;
 }
 
-// Replays a captured batch; false when its presized buffers overflowed (the
-// caller then runs the exact eager path).
+// Splits a batched call into groups of consecutive joins whose batch-level
+// per-record offsets (32-bit) and result sort keys (64-bit) fit; nearly
+// every batch is one group.
+std::vector<std::pair<int, int>> batch_groups(const fgss_sets_view* sets, int n) {
+    std::vector<std::pair<int, int>> g;
+    int b = 0;
+    uint64_t T = 0, R = 0, nmax = 0;
+    for (int i = 0; i < n; i++) {
+        const uint64_t t = sets[i].n_tokens, r = sets[i].n_sets, nm = std::max(nmax, r);
+        const bool fits = T + t < (1ull << 31) && R + r < (1ull << 31) && 2 * bits_for(nm) + bits_for(i - b + 1) <= 64;
+        if (!fits && i > b) {
+            g.push_back({b, i});
+            b = i;
+            T = R = nmax = 0;
+        }
+        T += t;
+        R += r;
+        nmax = std::max(nmax, r);
+    }
+    g.push_back({b, n});
+    return g;
+}
+
+// Replays a captured batch; false when its presized buffers are too small for
+// this call's data (the caller then runs the exact eager path).
 bool replay_graph(Ctx& c, GraphEntry& g, const fgss_sets_view* sets, const fgss_join_opts* opts, int n,
                   fgss_pairs* outs, fgss_stats* stats) {
     c.bpfx = g.ns;
     c.probe_timed = false;
+    std::vector<JoinState*> v;
+    for (auto& j : g.joins) v.push_back(j.get());
+    Batch& B = *g.batch;
     FGSS_CK(cudaEventRecord(c.ev[0], c.stream));
-    for (int i = 0; i < n; i++) {
-        // validation and fresh counters; the captured arguments (result buffers
-        // and capacities) stay as they were recorded
-        const JoinArgs saved = g.joins[i]->args;
-        join_setup(c, *g.joins[i], sets[i], opts[i], i, false);
-        g.joins[i]->args = saved;
+    // validation, fresh counters and the index and probe totals; the graph
+    // holds every later stage
+    batch_prep(c, B, v, sets, opts);
+    if (B.E > g.plan.E_cap || B.P > g.plan.P_cap) {
+        c.bpfx.clear();
+        return false;
     }
-    c.sync();
-    for (int i = 0; i < n; i++) join_check_input(c, *g.joins[i]);
     FGSS_CK(cudaEventRecord(c.ev[1], c.stream));
     FGSS_CK(cudaGraphLaunch(g.exec, c.stream));
     launch_counter() += g.launches;
     c.probe_timed = true;
     FGSS_CK(cudaEventRecord(c.ev[2], c.stream));
-    uint32_t* h = c.pinnedT<uint32_t>(g.ns + "h.st", 4 * (size_t)n + 4);
-    for (int i = 0; i < n; i++)
-        FGSS_CK(cudaMemcpyAsync(h + 4 * i, g.joins[i]->status, 16, cudaMemcpyDeviceToHost, c.stream));
+    uint32_t* h = c.pinnedT<uint32_t>(g.ns + "h.st", 8 * (size_t)n);
+    FGSS_CK(cudaMemcpyAsync(h, B.status, 32 * (size_t)n, cudaMemcpyDeviceToHost, c.stream));
     c.sync();
-    c.bpfx.clear();
     for (int i = 0; i < n; i++) {
         const uint32_t bad = ST_RES_OVERFLOW | ST_HEAVY_OVERFLOW | ST_HASH_FULL;
-        if ((h[4 * i] & bad) || h[4 * i + 3] > g.joins[i]->args.res_cap) return false;
+        if ((h[8 * i] & bad) || h[8 * i + 3] > g.plan.res_cap[i]) {
+            c.bpfx.clear();
+            return false;
+        }
     }
-    std::vector<JoinState*> v;
-    for (int i = 0; i < n; i++) {
-        JoinState& J = *g.joins[i];
-        J.n_res = h[4 * i + 3];
-        J.overflow_retries = 0;
-        join_finish_status(c, J);
-        export_pairs(c, J, opts[i], &outs[i]);
-        v.push_back(&J);
-    }
-    report_stats(c, v, stats, g.launches, n);
+    batch_finish_status(c, B);
+    c.bpfx.clear();
+    for (int i = 0; i < n; i++) v[i]->overflow_retries = 0;
+    export_batch(c, B, opts, outs);
+    Times t;
+    add_times(c, t);
+    report_stats(c, v, stats, g.launches, n, t);
     return true;
 }
 
@@ -266,7 +341,9 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
     bool batched = false;
     for (int i = 0; i < n; i++) batched |= opts[i].method == FGSS_METHOD_BATCHED;
     if (batched && opts[0].want_candidates) fail(FGSS_ERR_INVALID, "want_candidates needs the plain method");
-    bool graphable = batched && !c.tune_force && c.graphs;
+    const std::vector<std::pair<int, int>> groups =
+        batched ? batch_groups(sets, n) : std::vector<std::pair<int, int>>{{0, n}};
+    bool graphable = batched && !c.tune_force && c.graphs && groups.size() == 1;
     for (int i = 0; i < n; i++) graphable &= sets[i].on_device != 0 && !opts[i].no_graph;
     std::string gkey;
     std::unique_ptr<GraphEntry> g;
@@ -284,7 +361,6 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
                     throw;
                 }
                 if (ok) return;
-                for (int i = 0; i < n; i++) fgss_pairs_free(&outs[i]);
                 // its plan no longer fits the data: record a new one in the same buffers
                 cudaGraphExecDestroy(it->second->exec);
                 it->second->exec = nullptr;
@@ -299,47 +375,68 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
         c.bpfx = g->ns;
     }
     std::vector<std::unique_ptr<JoinState>> js(n);
+    std::vector<JoinState*> jv(n);
+    for (int i = 0; i < n; i++) {
+        js[i].reset(new JoinState());
+        js[i]->slot = i;
+        if (g) js[i]->ns = g->ns;
+        jv[i] = js[i].get();
+    }
     cudaEvent_t* ev = c.ev;
     const unsigned long long launches0 = launch_counter();
     c.probe_timed = false;
+    Times times;
     BatchPlan plan;
+    std::unique_ptr<Batch> Bp(new Batch());
     try {
-        FGSS_CK(cudaEventRecord(ev[0], c.stream));
-        for (int i = 0; i < n; i++) {
-            js[i].reset(new JoinState());
-            if (g) js[i]->ns = g->ns;
-            fgss_sets_view v = sets[i];
-            if (!v.on_device) {
-                // the same host arrays as an earlier join of the batch: copied to the device once
-                for (int j = 0; j < i; j++) {
-                    const fgss_sets_view& w = sets[j];
-                    if (!w.on_device && w.id == v.id && w.pos == v.pos && w.len == v.len && w.tokens == v.tokens &&
-                        w.n_sets == v.n_sets && w.n_tokens == v.n_tokens) {
-                        v = js[j]->in;
-                        v.n_terms = sets[i].n_terms;
-                        break;
+        if (!batched) {
+            FGSS_CK(cudaEventRecord(ev[0], c.stream));
+            for (int i = 0; i < n; i++) {
+                fgss_sets_view v = sets[i];
+                if (!v.on_device) {
+                    // the same host arrays as an earlier join of the batch: copied to the device once
+                    for (int j = 0; j < i; j++) {
+                        const fgss_sets_view& w = sets[j];
+                        if (!w.on_device && w.id == v.id && w.pos == v.pos && w.len == v.len &&
+                            w.tokens == v.tokens && w.n_sets == v.n_sets && w.n_tokens == v.n_tokens) {
+                            v = js[j]->in;
+                            v.n_terms = sets[i].n_terms;
+                            break;
+                        }
                     }
                 }
+                join_setup(c, *js[i], v, opts[i], i, false);
             }
-            join_setup(c, *js[i], v, opts[i], i, false);
-        }
-        c.sync();  // one wait for the whole batch's input validation
-        for (int i = 0; i < n; i++) join_check_input(c, *js[i]);
-        for (int i = 0; i < n; i++) join_index(c, *js[i]);
-        FGSS_CK(cudaEventRecord(ev[1], c.stream));
-        std::vector<JoinState*> v;
-        for (int i = 0; i < n; i++) v.push_back(js[i].get());
-        if (batched) {
-            batched_filter_verify(c, v, opts[0].use_model != 0, g ? &plan : nullptr);
-        } else {
+            c.sync();  // one wait for the whole batch's input validation
+            for (int i = 0; i < n; i++) join_check_input(c, *js[i]);
+            for (int i = 0; i < n; i++) join_index(c, *js[i]);
+            FGSS_CK(cudaEventRecord(ev[1], c.stream));
             for (int i = 0; i < n; i++) join_plain_filter_verify(c, *js[i], opts[i].want_candidates != 0);
+            FGSS_CK(cudaEventRecord(ev[2], c.stream));
+            for (int i = 0; i < n; i++) {
+                join_finish_status(c, *js[i]);
+                export_pairs(c, *js[i], opts[i], &outs[i]);
+            }
+            add_times(c, times);
+        } else {
+            for (const auto& gr : groups) {
+                Batch& B = *Bp;
+                std::vector<JoinState*> v;
+                for (int i = gr.first; i < gr.second; i++) v.push_back(jv[i]);
+                FGSS_CK(cudaEventRecord(ev[0], c.stream));
+                batch_prep(c, B, v, sets + gr.first, opts + gr.first);
+                plan.E_cap = B.E;
+                plan.P_cap = B.P;
+                batch_index(c, B, B.E);
+                FGSS_CK(cudaEventRecord(ev[1], c.stream));
+                batched_filter_verify(c, B, opts[gr.first].use_model != 0, g ? &plan : nullptr);
+                FGSS_CK(cudaEventRecord(ev[2], c.stream));
+                batch_finish_status(c, B);
+                export_batch(c, B, opts + gr.first, outs + gr.first);
+                add_times(c, times);
+            }
         }
-        FGSS_CK(cudaEventRecord(ev[2], c.stream));
-        for (int i = 0; i < n; i++) {
-            join_finish_status(c, *js[i]);
-            export_pairs(c, *js[i], opts[i], &outs[i]);
-        }
-        report_stats(c, v, stats, launch_counter() - launches0, n);
+        report_stats(c, jv, stats, launch_counter() - launches0, n, times);
         if (g && g->failed_captures < kMaxCaptureTries) {
             // capture the same batch (index build included) for later calls
             plan.capture = true;
@@ -348,8 +445,8 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
             FGSS_CK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
             bool captured = true;
             try {
-                for (int i = 0; i < n; i++) join_index(c, *js[i]);
-                batched_filter_verify(c, v, opts[0].use_model != 0, &plan);
+                batch_index(c, *Bp, plan.E_cap);
+                batched_filter_verify(c, *Bp, opts[0].use_model != 0, &plan);
             } catch (const Error& e) {
                 captured = false;  // this call's results stand; later calls run eagerly
                 if (c.verbose) fprintf(stderr, "[fgss] graph capture skipped: %s\n", e.msg.c_str());
@@ -367,6 +464,8 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
             launch_counter() = l0;  // captured, not launched
             if (captured) {
                 g->joins = std::move(js);
+                g->batch = std::move(Bp);
+                g->plan = plan;
             } else {
                 g->failed_captures++;  // later calls run eagerly in the same buffers
             }
@@ -629,18 +728,29 @@ fgss_status fgss_rsjoin(fgss_ctx* ctx, const fgss_sets_view* r, const fgss_sets_
         const RsInput u = rs_union(c, *r, *s);
         JoinState J;
         J.ns = "rs.";
-        join_setup(c, J, u.view, *opts, 0);
-        J.args.side = u.side;
-        join_index(c, J);
-        FGSS_CK(cudaEventRecord(ev[1], c.stream));
+        J.side = u.side;
         std::vector<JoinState*> v{&J};
-        if (opts->method == FGSS_METHOD_BATCHED) batched_filter_verify(c, v, opts->use_model != 0, nullptr);
-        else join_plain_filter_verify(c, J, false);
-        FGSS_CK(cudaEventRecord(ev[2], c.stream));
-        join_finish_status(c, J);
+        Batch B;
+        if (opts->method == FGSS_METHOD_BATCHED) {
+            batch_prep(c, B, v, &u.view, opts);
+            batch_index(c, B, B.E);
+            FGSS_CK(cudaEventRecord(ev[1], c.stream));
+            batched_filter_verify(c, B, opts->use_model != 0, nullptr);
+            FGSS_CK(cudaEventRecord(ev[2], c.stream));
+            batch_finish_status(c, B);
+        } else {
+            join_setup(c, J, u.view, *opts, 0);
+            join_index(c, J);
+            FGSS_CK(cudaEventRecord(ev[1], c.stream));
+            join_plain_filter_verify(c, J, false);
+            FGSS_CK(cudaEventRecord(ev[2], c.stream));
+            join_finish_status(c, J);
+        }
         rs_output(c, J, u);
         export_pairs(c, J, *opts, out);
-        report_stats(c, v, stats, launch_counter() - launches0, 1);
+        Times t;
+        add_times(c, t);
+        report_stats(c, v, stats, launch_counter() - launches0, 1, t);
     });
 }
 
@@ -934,9 +1044,11 @@ fgss_status fgss_query_costs(fgss_ctx* ctx, const fgss_sets_view* sets, const fg
         fgss_join_opts o = *opts;
         o.query_begin = o.query_end = 0;  // every query gets its estimate
         JoinState J;
-        join_setup(c, J, *sets, o, 0);
-        join_index(c, J);
-        join_query_costs(c, J, o.use_model != 0, costs);
+        std::vector<JoinState*> v{&J};
+        Batch B;
+        batch_prep(c, B, v, sets, &o);
+        batch_index(c, B, B.E);
+        batch_query_costs(c, B, o.use_model != 0, costs);
     });
 }
 

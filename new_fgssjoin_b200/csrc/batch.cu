@@ -1,95 +1,29 @@
-// batch.cu -- the batched method: per-query features and cost, balanced work
-// items, one persistent fused filter+verify launch over every join of a
-// batch, presized result buffers with an exact re-run on overflow.
+// batch.cu -- the batched method: every join of a batch in one launch per
+// stage (per-record counts, index, windows, bitmaps, chunk splits, features,
+// learned estimates, work-item costs, items, one persistent fused
+// filter+verify launch, one global-accumulator launch, result keys, sort,
+// output), presized result buffers with an exact re-run on overflow.
 #include <string.h>
 
 #include <algorithm>
 #include <cmath>
 
-#include "fused_kernels.cuh"
+#include "batch_kernels.cuh"
 #include "join.h"
 #include "model.h"
 #include "prims.cuh"
 
 namespace fgss {
 
-// Per query: features of the cost model and the heuristic cost
-// (sum of the probe tokens' full list lengths, plus the query size).
-__global__ void k_features(JoinArgs a, float t, float* __restrict__ feat, uint32_t* __restrict__ cost) {
+__global__ void k_widen(const uint32_t* in, uint64_t* out);
+static_assert(kFeatures == kFeat, "model feature rows");
+
+// Warp per record: the learned model's features of one join (training rows,
+// model_api.cu), the same as the batch's k_features_mj.
+__global__ void k_features(JoinArgs a, float* __restrict__ feat) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t lane = lane_id();
-    for (uint32_t q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < a.n; q += warps) {
-        uint32_t lq = a.len[q];
-        uint32_t qp = lq <= 65535u ? a.probe[lq] : 0;
-        const uint32_t* qt = a.tok + a.pos[q];
-        unsigned long long sum = 0;
-        uint32_t mx = 0;
-        float slog = 0.f;
-        for (uint32_t j = lane; j < qp; j += 32) {
-            uint32_t w = __ldg(qt + j);
-            uint32_t l = __ldg(a.list_off + w + 1) - __ldg(a.list_off + w);
-            sum += l;
-            mx = max(mx, l);
-            slog += log1pf((float)l);
-        }
-        sum = warp_sum(sum);
-        mx = __reduce_max_sync(kFull, mx);
-        slog = warp_sum(slog);
-        if (lane == 0) {
-            uint32_t send = lq <= 65535u ? a.send[lq] : q + 1;
-            uint32_t win = send > q + 1 ? send - q - 1 : 0;
-            float* f = feat + (uint64_t)q * kFeat;
-            f[0] = log1pf((float)lq);
-            f[1] = log1pf((float)qp);
-            f[2] = log1pf((float)sum);
-            f[3] = log1pf((float)mx);
-            f[4] = qp ? slog / (float)qp : 0.f;
-            f[5] = log1pf((float)win);
-            f[6] = a.n ? (float)q / (float)a.n : 0.f;
-            f[7] = t;
-            unsigned long long c = sum + lq;
-            cost[q] = (uint32_t)min(c, 0x3fffffffull);
-        }
-    }
-}
-
-// Work items of one join: item k = queries with exclusive cost prefix in
-// [k*target, (k+1)*target).
-__global__ void k_items(const uint64_t* __restrict__ pre, uint32_t n, const uint64_t* __restrict__ d_total, uint32_t K,
-                        uint32_t join, uint4* __restrict__ items) {
-    const uint64_t total = *d_total;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
-        uint64_t target = (total + K - 1) / K;
-        auto first_ge = [&](uint64_t x) {
-            uint32_t lo = 0, hi = n;
-            while (lo < hi) {
-                uint32_t mid = (lo + hi) >> 1;
-                if (pre[mid] < x) lo = mid + 1;
-                else hi = mid;
-            }
-            return lo;
-        };
-        uint32_t b = k == 0 ? 0 : first_ge(k * target);
-        uint32_t e = k + 1 == K ? n : first_ge((k + 1) * target);
-        items[k] = make_uint4(join, b, max(b, e), 0);
-    }
-}
-
-// Item sort keys: ~cost (so ascending order = descending cost), value = item index.
-// Sort key of a work item: its cost as a float's exponent and top 7 mantissa
-// bits (the longest-first order needs no more), complemented so an ascending
-// sort puts the costliest first; 16 bits, two radix passes.
-__global__ void k_item_keys(const uint64_t* __restrict__ pre, uint32_t n, const uint64_t* __restrict__ d_total,
-                            const uint4* __restrict__ items, uint32_t K, uint32_t base, uint32_t* __restrict__ key,
-                            uint32_t* __restrict__ val) {
-    const uint64_t total = *d_total;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
-        const uint4 it = items[k];
-        const uint64_t b = it.y < n ? pre[it.y] : total;
-        const uint64_t e = it.z < n ? pre[it.z] : total;
-        key[base + k] = (~__float_as_uint((float)(e - b)) >> 16) & 0xffffu;
-        val[base + k] = base + k;
-    }
+    for (uint32_t q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < a.n; q += warps)
+        features_record(a, q, feat + (uint64_t)q * kFeatures);
 }
 
 __global__ void k_permute_items(const uint4* __restrict__ items, const uint32_t* __restrict__ order, uint64_t n,
@@ -193,339 +127,525 @@ void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const Fus
     else launch_fused<64, 9, 768, false>(c, d_args, d_fargs, items, n_items, counter, te.ctas_per_sm);
 }
 
-// Work-item cost of a query: exact window entries + a verification estimate.
-__global__ void k_cost(const uint32_t* __restrict__ wtot, const uint32_t* __restrict__ len,
-                       const uint32_t* __restrict__ pred_cand, uint32_t n, uint32_t q_lo, uint32_t q_hi,
-                       uint64_t* __restrict__ cost) {
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        if (q < q_lo || q >= q_hi) {  // outside this shard: no work
-            cost[q] = 0;
-            continue;
-        }
-        unsigned long long v = (unsigned long long)wtot[q] + len[q];
-        if (pred_cand) v += 4ull * pred_cand[q];
-        cost[q] = v;
+namespace {
+
+constexpr uint32_t kRecTile = 256;  // records per tile of the per-record stages (thread per record in the MLP)
+
+// Uploads the tile map of joins [off[j], off[j+1]) in tiles of `tile` to the
+// device buffer `name` (through a pinned buffer of its own, so a captured
+// graph's copy node always reads this map).
+TileMap upload_tiles(Ctx& c, const std::string& name, const std::vector<uint64_t>& off, uint32_t tile) {
+    const size_t nj = off.size() - 1;
+    const size_t bytes = (nj + 1) * 12;
+    char* h = (char*)c.pinned(name + ".h", bytes);
+    uint64_t* ho = reinterpret_cast<uint64_t*>(h);
+    uint32_t* ht = reinterpret_cast<uint32_t*>(h + (nj + 1) * 8);
+    uint64_t t = 0;
+    for (size_t j = 0; j < nj; j++) {
+        ho[j] = off[j];
+        ht[j] = (uint32_t)t;
+        t += (off[j + 1] - off[j] + tile - 1) / tile;
     }
+    ho[nj] = off[nj];
+    if (t >= 0xffffffffull) fail(FGSS_ERR_UNSUPPORTED, "too many tiles in one batch");
+    ht[nj] = (uint32_t)t;
+    char* d = (char*)c.dev(name, bytes);
+    FGSS_CK(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, c.stream));
+    TileMap m;
+    m.roff = reinterpret_cast<const uint64_t*>(d);
+    m.tile_off = reinterpret_cast<const uint32_t*>(d + (nj + 1) * 8);
+    m.nj = (uint32_t)nj;
+    m.tile = tile;
+    m.ntiles = (uint32_t)t;
+    return m;
 }
 
-// Resets the filter's counters and overflow bit of one join before a re-run
-// (the input-validation bits and the probe-token count stay).
-__global__ void k_clear_filter_state(uint32_t* status, unsigned long long* stats) {
-    if (threadIdx.x == 0) {
-        status[0] &= ~(uint32_t)(ST_RES_OVERFLOW | ST_HEAVY_OVERFLOW | ST_HASH_FULL);
-        status[2] = 0;
-        status[3] = 0;
-    }
-    if (threadIdx.x < SS_N && threadIdx.x != SS_PROBE) stats[threadIdx.x] = 0;
+// Every join's JoinArgs to the device, through the pinned buffer `name`.
+void upload_args(Ctx& c, Batch& B, const std::string& name) {
+    const size_t nj = B.js.size();
+    JoinArgs* h = c.pinnedT<JoinArgs>(name, nj);
+    for (size_t j = 0; j < nj; j++) h[j] = B.js[j]->args;
+    FGSS_CK(cudaMemcpyAsync(B.d_args, h, nj * sizeof(JoinArgs), cudaMemcpyHostToDevice, c.stream));
 }
 
-// The batched method's pre-pass of one join (index built already): windows of
-// every probe token (exact per-query work), bitmaps, chunk splits for slot
-// tables of cap_entries, the learned model's estimates (use_model), and the
-// work-item cost of every query (window entries + 4 x predicted candidates +
-// size) with its exclusive prefix in `pre` and total in d_total.
-FusedArgs join_prepass(Ctx& c, JoinState& J, uint32_t cap_entries, bool use_model, uint64_t* d_pred_res,
-                       uint64_t* d_pred_cand, uint64_t* pre, uint64_t* d_total) {
-    const uint64_t n = J.in.n_sets;
-    float* feat = c.devT<float>(J.pfx("feat"), (n + 1) * kFeat);
-    uint64_t* cost = c.devT<uint64_t>(J.pfx("cost"), n + 1);
-    uint32_t* fcost = c.devT<uint32_t>(J.pfx("fcost"), n + 1);
-    uint32_t* poff = c.devT<uint32_t>(J.pfx("poff"), n + 1);
-    uint2* win = c.devT<uint2>(J.pfx("win"), J.in.n_tokens + 1);
-    uint32_t* wpre = c.devT<uint32_t>(J.pfx("wpre"), J.in.n_tokens + 1);
-    uint32_t* wtot = c.devT<uint32_t>(J.pfx("wtot"), n + 1);
-    uint32_t* pred = c.devT<uint32_t>(J.pfx("pred"), n + 1);
-    uint4* meta = c.devT<uint4>(J.pfx("meta"), n + 1);
-    const uint32_t bmw = bitmap_words(J.in.n_tokens, n);
-    uint4* bmap = c.devT<uint4>(J.pfx("bmap"), (uint64_t)bmw * n + 4);
-    uint2* qchunk = c.devT<uint2>(J.pfx("qchunk"), n + 1);
-    const uint64_t cbuf_cap = 2 * J.in.n_tokens + (1u << 20);  // overflowing queries bisect instead
-    uint32_t* cbuf = c.devT<uint32_t>(J.pfx("cbuf"), cbuf_cap);
-    FusedArgs f;
-    f.poff = poff;
-    f.win = win;
-    f.wpre = wpre;
-    f.smin = J.lut.smin;
-    f.meta = meta;
-    f.qchunk = qchunk;
-    f.cbuf = cbuf;
-    f.bmap = bmap;
-    f.bmw = bmw;
-    J.d_cost = cost;
-    if (n == 0) return f;
-    // windows of every probe token (exact per-query work), chunk splits, then
-    // features and the learned estimate, then the work-item cost prefix
-    exclusive_scan<uint32_t>(c, J.pcnt, poff, n, nullptr, (uint32_t*)nullptr, J.pfx("scan.p").c_str());
-    unsigned long long* cused = reinterpret_cast<unsigned long long*>(J.status + 4);
+unsigned tile_grid(Ctx& c, const TileMap& m, unsigned per_sm = 16) {
+    return std::max<unsigned>(1, std::min<unsigned>(m.ntiles, (unsigned)c.num_sms * per_sm));
+}
+
+template <typename K>
+void index_sort(Ctx& c, Batch& B, uint64_t E_cap, int tbits, int jbits, const uint64_t* d_E, const uint64_t* d_loff,
+                uint32_t* list, uint32_t* ent_s, uint32_t* ent_pl) {
+    const std::string& p = c.bpfx;
+    K* key = c.devT<K>(p + "b.ix.key", E_cap + 1);
+    uint64_t* val = c.devT<uint64_t>(p + "b.ix.val", E_cap + 1);
+    k_index_entries_mj<K><<<tile_grid(c, B.rec), 256, 0, c.stream>>>(B.d_args, B.rec, B.ioff, (uint32_t)tbits, key,
+                                                                      val);
+    FGSS_LAUNCH_CK();
+    radix_sort<K, uint64_t>(c, key, val, E_cap, d_E, 0, tbits + jbits, (p + "b.ixsort").c_str());
+    k_index_lists_mj<K><<<grid_for(E_cap, 256, c.num_sms * 32), 256, 0, c.stream>>>(
+        B.d_args, key, val, d_E, (uint32_t)tbits, d_loff, list, ent_s, ent_pl);
+    FGSS_LAUNCH_CK();
+}
+
+// The batch's pre-pass (index built): windows of every probe token (exact
+// per-query work), bitmaps, chunk splits for slot tables of cap_entries, the
+// learned model's estimates (model) and the work-item cost of every query
+// (window entries + 4 x predicted candidates + size) with its exclusive
+// prefix in cpre (total at cpre[R]).  d_sums: [0, nj) cost totals,
+// [nj, 2nj) predicted results, [2nj, 3nj) predicted candidates.
+struct Prepass {
+    FusedArgs* d_fargs = nullptr;
+    uint64_t* cost = nullptr;
+    uint64_t* cpre = nullptr;
+    uint64_t* d_sums = nullptr;
+};
+
+Prepass batch_prepass(Ctx& c, Batch& B, uint32_t cap_entries, uint64_t P_cap, bool model) {
+    const size_t nj = B.js.size();
+    const std::string& p = c.bpfx;
+    const uint64_t R = B.R;
+    uint2* win = c.devT<uint2>(p + "b.win", P_cap + 1);
+    uint32_t* wpre = c.devT<uint32_t>(p + "b.wpre", P_cap + 1);
+    uint32_t* wtot = c.devT<uint32_t>(p + "b.wtot", R + 1);
+    uint4* meta = c.devT<uint4>(p + "b.meta", R + 1);
+    uint2* qchunk = c.devT<uint2>(p + "b.qchunk", R + 1);
+    const uint64_t cbuf_cap = 2 * P_cap + (1u << 20);  // overflowing queries bisect instead
+    uint32_t* cbuf = c.devT<uint32_t>(p + "b.cbuf", cbuf_cap);
+    std::vector<uint64_t> boff(nj + 1, 0);
+    std::vector<uint32_t> bmw(nj);
+    for (size_t j = 0; j < nj; j++) {
+        bmw[j] = bitmap_words(B.js[j]->in.n_tokens, B.js[j]->in.n_sets);
+        boff[j + 1] = boff[j] + (uint64_t)bmw[j] * B.js[j]->in.n_sets;
+    }
+    uint4* bmap = c.devT<uint4>(p + "b.bmap", boff[nj] + 4);
+    FusedArgs* hf = c.pinnedT<FusedArgs>(p + "b.hf", nj);
+    for (size_t j = 0; j < nj; j++) {
+        FusedArgs& f = hf[j];
+        f.poff = B.poff + B.roff[j];
+        f.win = win;
+        f.wpre = wpre;
+        f.smin = B.js[j]->lut.smin;
+        f.meta = meta + B.roff[j];
+        f.qchunk = qchunk + B.roff[j];
+        f.cbuf = cbuf;
+        f.bmap = bmap + boff[j];
+        f.bmw = bmw[j];
+    }
+    Prepass pp;
+    pp.d_fargs = c.devT<FusedArgs>(p + "b.fargs", nj);
+    FGSS_CK(cudaMemcpyAsync(pp.d_fargs, hf, nj * sizeof(FusedArgs), cudaMemcpyHostToDevice, c.stream));
+    unsigned long long* cused = c.devT<unsigned long long>(p + "b.cused", 1);
     FGSS_CK(cudaMemsetAsync(cused, 0, 8, c.stream));
-    k_windows<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wpre, wtot, meta);
+    float* feat = c.devT<float>(p + "b.feat", (R + 1) * kFeatures);
+    uint32_t* pred = c.devT<uint32_t>(p + "b.pred", R + 1);
+    pp.cost = c.devT<uint64_t>(p + "b.cost", R + 1);
+    pp.cpre = c.devT<uint64_t>(p + "b.cpre", R + 1);
+    pp.d_sums = c.devT<uint64_t>(p + "b.sums", 3 * nj + 2);
+    FGSS_CK(cudaMemsetAsync(pp.d_sums, 0, (3 * nj + 2) * 8, c.stream));
+    if (R == 0) return pp;
+    const unsigned g = tile_grid(c, B.rec);
+    k_windows_mj<<<g, 256, 0, c.stream>>>(B.d_args, B.rec, B.poff, win, wpre, wtot, meta);
     FGSS_LAUNCH_CK();
-    k_bitmaps<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, bmap, bmw);
+    k_bitmaps_mj<<<g, 256, 0, c.stream>>>(B.d_args, pp.d_fargs, B.rec);
     FGSS_LAUNCH_CK();
-    k_chunks<<<grid_for(n * 32, 256, c.num_sms * 64), 256, 0, c.stream>>>(J.args, poff, win, wtot, cap_entries, qchunk,
-                                                                        cbuf, cbuf_cap, cused);
+    k_chunks_mj<<<g, 256, 0, c.stream>>>(B.d_args, pp.d_fargs, B.rec, wtot, cap_entries, cbuf, cbuf_cap, cused);
     FGSS_LAUNCH_CK();
-    const bool model = use_model && c.model && !J.res_cap_hint;
     if (model) {
-        k_features<<<grid_for(n * 32, 256, c.num_sms * 32), 256, 0, c.stream>>>(J.args, J.t, feat, fcost);
+        k_features_mj<<<g, 256, 0, c.stream>>>(B.d_args, B.rec, feat);
         FGSS_LAUNCH_CK();
-        model_predict(c, feat, n, pred, d_pred_res, d_pred_cand);
+        model_predict_tiles(c, feat, B.rec, pred, pp.d_sums + nj, pp.d_sums + 2 * nj);
     }
-    k_cost<<<grid_for(n, 256, c.num_sms * 8), 256, 0, c.stream>>>(wtot, J.in.len, model ? pred : nullptr, (uint32_t)n,
-                                                                   J.args.q_lo, J.args.q_hi, cost);
+    k_cost_mj<<<g, 256, 0, c.stream>>>(B.d_args, B.rec, wtot, model ? pred : nullptr, pp.cost);
     FGSS_LAUNCH_CK();
-    exclusive_scan<uint64_t>(c, cost, pre, n, nullptr, d_total, J.pfx("scan.cost").c_str());
-    return f;
+    exclusive_scan<uint64_t>(c, pp.cost, pp.cpre, R, nullptr, pp.cpre + R, (p + "b.scan.c").c_str());
+    k_join_cost_totals<<<grid_for(nj, 128), 128, 0, c.stream>>>(B.rec.roff, (uint32_t)nj, pp.cpre, pp.d_sums);
+    FGSS_LAUNCH_CK();
+    return pp;
 }
 
-// Per-query work estimates of one join (index built already), to host `out`:
-// the costs the batched method balances its work items by.
-void join_query_costs(Ctx& c, JoinState& J, bool use_model, uint64_t* out) {
-    const uint64_t n = J.in.n_sets;
-    if (n == 0) return;
-    const TuneEntry te = tune_lookup(c, tune_key(n, J.in.n_tokens, J.t));
-    uint64_t* d_tot = c.devT<uint64_t>(J.pfx("qc.tot"), 4);
-    FGSS_CK(cudaMemsetAsync(d_tot, 0, 32, c.stream));
-    uint64_t* pre = c.devT<uint64_t>(J.pfx("cpre"), n + 1);
-    join_prepass(c, J, (1u << te.hash_log2) / 2, use_model, d_tot + 1, d_tot + 2, pre, d_tot);
-    FGSS_CK(cudaMemcpyAsync(out, J.d_cost, n * 8, cudaMemcpyDeviceToHost, c.stream));
+// The batch's launch shape: the tuned shape of its most expensive join (the
+// lowest threshold, then the most records), or the one of a requested strategy.
+TuneEntry batch_shape(Ctx& c, const Batch& B) {
+    if (c.tune_force) return *c.tune_force;
+    size_t lead = 0;
+    for (size_t i = 1; i < B.js.size(); i++)
+        if (B.js[i]->t < B.js[lead]->t || (B.js[i]->t == B.js[lead]->t && B.js[i]->in.n_sets > B.js[lead]->in.n_sets))
+            lead = i;
+    const JoinState& L = *B.js[lead];
+    if (L.filter != FGSS_FILTER_AUTO) return filter_entry(L.filter);
+    return tune_lookup(c, tune_key(L.in.n_sets, L.in.n_tokens, L.t));
+}
+
+}  // namespace
+
+void batch_prep(Ctx& c, Batch& B, const std::vector<JoinState*>& js, const fgss_sets_view* views,
+                const fgss_join_opts* opts) {
+    const size_t nj = js.size();
+    const std::string& p = c.bpfx;
+    B.js = js;
+    B.roff.assign(nj + 1, 0);
+    B.n_max = 0;
+    B.terms_max = 0;
+    uint64_t T = 0;
+    for (size_t j = 0; j < nj; j++) {
+        JoinState& J = *js[j];
+        fgss_sets_view v = views[j];
+        if (!v.on_device) {
+            // the same host arrays as an earlier join of the batch: copied to the device once
+            for (size_t k = 0; k < j; k++) {
+                const fgss_sets_view& w = views[k];
+                if (!w.on_device && w.id == v.id && w.pos == v.pos && w.len == v.len && w.tokens == v.tokens &&
+                    w.n_sets == v.n_sets && w.n_tokens == v.n_tokens) {
+                    v = js[k]->in;
+                    v.n_terms = views[j].n_terms;
+                    break;
+                }
+            }
+        }
+        join_setup_host(c, J, v, opts[j], J.slot);
+        B.roff[j + 1] = B.roff[j] + J.in.n_sets;
+        B.n_max = std::max<uint32_t>(B.n_max, (uint32_t)J.in.n_sets);
+        B.terms_max = std::max<uint32_t>(B.terms_max, J.in.n_terms);
+        T += J.in.n_tokens;
+    }
+    B.R = B.roff[nj];
+    // per-record offsets are 32-bit: the caller splits larger batches
+    if (T >= 0xffffffffull || B.R >= 0xffffffffull) fail(FGSS_ERR_UNSUPPORTED, "a batch of 2^32 or more tokens");
+    B.status = c.devT<uint32_t>(p + "b.status", nj * 8);
+    B.stats = c.devT<unsigned long long>(p + "b.stats", nj * SS_N);
+    B.d_e = c.devT<uint64_t>(p + "b.E", nj * 2);
+    B.icnt = c.devT<uint32_t>(p + "b.icnt", B.R + 1);
+    B.pcnt = c.devT<uint32_t>(p + "b.pcnt", B.R + 1);
+    B.ioff = c.devT<uint32_t>(p + "b.ioff", B.R + 1);
+    B.poff = c.devT<uint32_t>(p + "b.poff", B.R + 1);
+    B.send = c.devT<uint32_t>(p + "b.send", nj * 65537);
+    B.heavy_q = c.devT<uint32_t>(p + "b.heavy_q", B.R + 1);
+    B.d_args = c.devT<JoinArgs>(p + "b.args", nj);
+    FGSS_CK(cudaMemsetAsync(B.status, 0, nj * 32, c.stream));
+    FGSS_CK(cudaMemsetAsync(B.stats, 0, nj * SS_N * 8, c.stream));
+    for (size_t j = 0; j < nj; j++) {
+        JoinState& J = *js[j];
+        J.status = B.status + 8 * j;
+        J.stats = B.stats + SS_N * j;
+        J.maxlen = J.status + 1;
+        J.d_e = B.d_e + 2 * j;
+        J.icnt = B.icnt + B.roff[j];
+        J.pcnt = B.pcnt + B.roff[j];
+        JoinArgs& a = J.args;
+        a.status = J.status;
+        a.stats = J.stats;
+        a.send = B.send + 65537ull * j;
+        a.heavy_q = B.heavy_q + B.roff[j];
+        a.heavy_count = J.status + 2;
+        a.res_count = J.status + 3;
+    }
+    B.rec = upload_tiles(c, p + "b.rec", B.roff, kRecTile);
+    upload_args(c, B, p + "b.ha0");
+    if (B.R) {
+        k_prep_mj<<<tile_grid(c, B.rec), 256, 0, c.stream>>>(B.d_args, B.rec, B.icnt, B.pcnt);
+        FGSS_LAUNCH_CK();
+        k_send_mj<<<grid_for((uint64_t)nj << 16, 256, c.num_sms * 32), 256, 0, c.stream>>>(B.d_args, (uint32_t)nj,
+                                                                                          B.send);
+        FGSS_LAUNCH_CK();
+        exclusive_scan<uint32_t>(c, B.icnt, B.ioff, B.R, nullptr, B.ioff + B.R, (p + "b.scan.i").c_str());
+        exclusive_scan<uint32_t>(c, B.pcnt, B.poff, B.R, nullptr, B.poff + B.R, (p + "b.scan.p").c_str());
+    } else {
+        FGSS_CK(cudaMemsetAsync(B.ioff, 0, 4, c.stream));
+        FGSS_CK(cudaMemsetAsync(B.poff, 0, 4, c.stream));
+    }
+    // one wait for the whole batch: no kernel reads tokens through caller
+    // offsets before they are validated
+    uint32_t* h = c.pinnedT<uint32_t>(p + "b.hprep", nj * 8 + 2);
+    FGSS_CK(cudaMemcpyAsync(h, B.status, nj * 32, cudaMemcpyDeviceToHost, c.stream));
+    FGSS_CK(cudaMemcpyAsync(h + nj * 8, B.ioff + B.R, 4, cudaMemcpyDeviceToHost, c.stream));
+    FGSS_CK(cudaMemcpyAsync(h + nj * 8 + 1, B.poff + B.R, 4, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    for (size_t j = 0; j < nj; j++)
+        if (js[j]->in.n_sets) check_input_status(h[8 * j]);
+    B.E = h[nj * 8];
+    B.P = h[nj * 8 + 1];
+}
+
+void batch_index(Ctx& c, Batch& B, uint64_t E_cap) {
+    const size_t nj = B.js.size();
+    const std::string& p = c.bpfx;
+    if (E_cap < B.E) fail(FGSS_ERR_CUDA, "index buffers below the batch's entry count");
+    const int tbits = bits_for((uint64_t)B.terms_max + 1);
+    const int jbits = bits_for(nj);
+    // join j's list offsets: n_terms + 1 entries from loff[j], positions in
+    // the batch's entry arrays
+    uint64_t* hl = c.pinnedT<uint64_t>(p + "b.hloff", nj + 1);
+    hl[0] = 0;
+    for (size_t j = 0; j < nj; j++) hl[j + 1] = hl[j] + B.js[j]->in.n_terms + 1;
+    const uint64_t L = hl[nj];
+    uint64_t* d_loff = c.devT<uint64_t>(p + "b.loff", nj + 1);
+    FGSS_CK(cudaMemcpyAsync(d_loff, hl, (nj + 1) * 8, cudaMemcpyHostToDevice, c.stream));
+    uint32_t* list = c.devT<uint32_t>(p + "b.list", L + 1);
+    uint32_t* ent_s = c.devT<uint32_t>(p + "b.ent_s", E_cap + 1);
+    uint32_t* ent_pl = c.devT<uint32_t>(p + "b.ent_pl", E_cap + 1);
+    for (size_t j = 0; j < nj; j++) {
+        JoinArgs& a = B.js[j]->args;
+        a.list_off = list + hl[j];
+        a.ent_s = ent_s;
+        a.ent_pl = ent_pl;
+    }
+    // a join without entries keeps these zero offsets (empty lists)
+    FGSS_CK(cudaMemsetAsync(list, 0, L * 4, c.stream));
+    FGSS_CK(cudaMemsetAsync(B.d_e, 0, nj * 16, c.stream));
+    if (B.R) {
+        uint64_t* d_E = c.devT<uint64_t>(p + "b.dE", 2);
+        k_widen<<<1, 1, 0, c.stream>>>(B.ioff + B.R, d_E);
+        FGSS_LAUNCH_CK();
+        k_join_entries<<<grid_for(nj, 128), 128, 0, c.stream>>>(B.rec.roff, (uint32_t)nj, B.ioff, B.d_e);
+        FGSS_LAUNCH_CK();
+        if (tbits + jbits <= 32) index_sort<uint32_t>(c, B, E_cap, tbits, jbits, d_E, d_loff, list, ent_s, ent_pl);
+        else index_sort<uint64_t>(c, B, E_cap, tbits, jbits, d_E, d_loff, list, ent_s, ent_pl);
+    }
+    upload_args(c, B, p + "b.ha1");
+}
+
+void batch_query_costs(Ctx& c, Batch& B, bool use_model, uint64_t* out) {
+    if (B.R == 0) return;
+    const TuneEntry te = batch_shape(c, B);
+    const Prepass pp = batch_prepass(c, B, (1u << te.hash_log2) / 2, B.P, use_model && c.model);
+    FGSS_CK(cudaMemcpyAsync(out, pp.cost, B.R * 8, cudaMemcpyDeviceToHost, c.stream));
     c.sync();
 }
 
-// Runs the fused filter+verify over every join (their index built already).
+// Runs the fused filter+verify over every join of the batch (index built).
 //
 // With a plan in record mode the host-side decisions of this run (launch
-// shape, work items per join, result capacities, heavy-path slots, grid) are
-// kept; in capture mode (plan->capture) the same device work is issued with
-// those decisions and without any host synchronization, so the stream can be
-// captured into a CUDA graph and replayed on later calls.
-void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_model, BatchPlan* plan) {
-    const size_t nj = joins.size();
+// shape, buffer sizes, work items per join, result capacities, heavy-path
+// slots) are kept; in capture mode (plan->capture) the same device work is
+// issued with those decisions and without any host synchronization, so the
+// stream can be captured into a CUDA graph and replayed on later calls.
+void batched_filter_verify(Ctx& c, Batch& B, bool use_model, BatchPlan* plan) {
+    const size_t nj = B.js.size();
+    std::vector<JoinState*>& joins = B.js;
     const bool capture = plan && plan->capture;
-    // d_tot: [0, nj) cost totals, [nj, 2nj) predicted results, [2nj, 3nj) predicted candidates
-    uint64_t* d_tot = c.devT<uint64_t>(c.bpfx + "b.tot", nj * 3 + 2);
-    std::vector<uint64_t*> pre(nj);
-    FGSS_CK(cudaMemsetAsync(d_tot, 0, (nj * 3 + 2) * 8, c.stream));
-    FusedArgs* hf = c.pinnedT<FusedArgs>(c.bpfx + "b.hf", nj);
-    TuneEntry te;
-    if (capture) {
-        te = plan->te;
-    } else {
-        // one launch shape for the batch: the tuned shape of its most expensive
-        // join (the lowest threshold, then the most records)
-        size_t lead = 0;
-        for (size_t i = 1; i < nj; i++)
-            if (joins[i]->t < joins[lead]->t ||
-                (joins[i]->t == joins[lead]->t && joins[i]->in.n_sets > joins[lead]->in.n_sets))
-                lead = i;
-        te = c.tune_force ? *c.tune_force
-                          : tune_lookup(c, tune_key(joins[lead]->in.n_sets, joins[lead]->in.n_tokens, joins[lead]->t));
-        if (!c.tune_force && joins[lead]->filter != FGSS_FILTER_AUTO) te = filter_entry(joins[lead]->filter);
-    }
+    const std::string& p = c.bpfx;
+    const TuneEntry te = capture ? plan->te : batch_shape(c, B);
     const uint32_t cap_entries = (1u << te.hash_log2) / 2;  // chunk capacity of the chosen kernel shape
-    for (size_t i = 0; i < nj; i++) {
-        JoinState& J = *joins[i];
-        pre[i] = c.devT<uint64_t>(J.pfx("cpre"), J.in.n_sets + 1);
-        hf[i] = join_prepass(c, J, cap_entries, use_model, &d_tot[nj + i], &d_tot[2 * nj + i], pre[i], &d_tot[i]);
-    }
-    FusedArgs* d_fargs = c.devT<FusedArgs>(c.bpfx + "b.fargs", nj);
-    FGSS_CK(cudaMemcpyAsync(d_fargs, hf, nj * sizeof(FusedArgs), cudaMemcpyHostToDevice, c.stream));
+    const uint64_t P_cap = plan ? plan->P_cap : B.P;
+    if (P_cap < B.P) fail(FGSS_ERR_CUDA, "window buffers below the batch's probe-token count");
+    const bool model = use_model && c.model;
+    const Prepass pp = batch_prepass(c, B, cap_entries, P_cap, model);
+
+    // work items: ~256 per resident CTA over the whole batch (a few queries per
+    // item at 100k records), split by cost share and handed out longest first,
+    // so the dynamic queue ends with short items
     std::vector<uint32_t> K(nj, 0);
     uint64_t nitems = 0;
-    std::vector<uint64_t> htot(3 * nj + 2, 0);
+    uint64_t* hsum = c.pinnedT<uint64_t>(p + "b.hsum", 3 * nj + 2);
     if (capture) {
         K = plan->K;
         nitems = plan->nitems;
     } else {
-        FGSS_CK(cudaMemcpyAsync(htot.data(), d_tot, (3 * nj + 2) * 8, cudaMemcpyDeviceToHost, c.stream));
+        FGSS_CK(cudaMemcpyAsync(hsum, pp.d_sums, (3 * nj + 2) * 8, cudaMemcpyDeviceToHost, c.stream));
         c.sync();
         for (size_t i = 0; i < nj; i++) {
-            if (!(use_model && c.model && !joins[i]->res_cap_hint)) continue;
-            joins[i]->pred_results = htot[nj + i];
-            joins[i]->pred_candidates = htot[2 * nj + i];
+            if (!model || joins[i]->res_cap_hint) continue;
+            joins[i]->pred_results = hsum[nj + i];
+            joins[i]->pred_candidates = hsum[2 * nj + i];
         }
         uint64_t grand = 0;
-        for (size_t i = 0; i < nj; i++) grand += htot[i];
-        // ~256 items per resident CTA over the whole batch (a few queries per item at
-        // 100k records), split by cost share and handed out longest first, so the
-        // dynamic queue ends with short items
+        for (size_t i = 0; i < nj; i++) grand += hsum[i];
         const uint64_t want = (uint64_t)256 * fused_resident_ctas(c, te);
         for (size_t i = 0; i < nj; i++) {
             const uint64_t n = joins[i]->in.n_sets;
             if (n == 0) continue;
-            uint64_t k = grand ? (want * htot[i] + grand - 1) / grand : 1;
+            uint64_t k = grand ? (want * hsum[i] + grand - 1) / grand : 1;
             k = std::max<uint64_t>(1, std::min<uint64_t>(k, n));
             K[i] = (uint32_t)k;
             nitems += k;
         }
     }
-    uint4* items = c.devT<uint4>(c.bpfx + "b.items", nitems + 1);
-    uint64_t off = 0;
-    for (size_t i = 0; i < nj; i++) {
-        if (!K[i]) continue;
-        JoinState& J = *joins[i];
-        k_items<<<grid_for(K[i], 128), 128, 0, c.stream>>>(pre[i], (uint32_t)J.in.n_sets, &d_tot[i], K[i],
-                                                            (uint32_t)i, items + off);
+    if (nitems >= 0xffffffffull) fail(FGSS_ERR_UNSUPPORTED, "too many work items");
+    uint32_t* hk = c.pinnedT<uint32_t>(p + "b.hkoff", nj + 1);
+    hk[0] = 0;
+    for (size_t i = 0; i < nj; i++) hk[i + 1] = hk[i] + K[i];
+    uint32_t* d_koff = c.devT<uint32_t>(p + "b.koff", nj + 1);
+    FGSS_CK(cudaMemcpyAsync(d_koff, hk, (nj + 1) * 4, cudaMemcpyHostToDevice, c.stream));
+    uint4* items = c.devT<uint4>(p + "b.items", nitems + 1);
+    if (nitems) {
+        uint32_t* ikey = c.devT<uint32_t>(p + "b.ikey", nitems + 1);
+        uint32_t* ival = c.devT<uint32_t>(p + "b.ival", nitems + 1);
+        k_items_mj<<<grid_for(nitems, 128), 128, 0, c.stream>>>(B.rec.roff, d_koff, (uint32_t)nj, (uint32_t)nitems,
+                                                                 pp.cpre, pp.d_sums, items, ikey, ival);
         FGSS_LAUNCH_CK();
-        off += K[i];
-    }
-    if (nitems > 1) {
-        // longest-processing-time order: sort items by descending cost
-        uint32_t* ikey = c.devT<uint32_t>(c.bpfx + "b.ikey", nitems + 1);
-        uint32_t* ival = c.devT<uint32_t>(c.bpfx + "b.ival", nitems + 1);
-        uint4* sorted = c.devT<uint4>(c.bpfx + "b.items2", nitems + 1);
-        uint64_t off2 = 0;
-        for (size_t i = 0; i < nj; i++) {
-            if (!K[i]) continue;
-            k_item_keys<<<grid_for(K[i], 128), 128, 0, c.stream>>>(pre[i], (uint32_t)joins[i]->in.n_sets, &d_tot[i],
-                                                                    items + off2, K[i], (uint32_t)off2, ikey, ival);
+        if (nitems > 1) {
+            // longest-processing-time order: sort items by descending cost
+            uint4* sorted = c.devT<uint4>(p + "b.items2", nitems + 1);
+            radix_sort<uint32_t, uint32_t>(c, ikey, ival, nitems, nullptr, 0, 16, (p + "b.isort").c_str());
+            k_permute_items<<<grid_for(nitems, 128), 128, 0, c.stream>>>(items, ival, nitems, sorted);
             FGSS_LAUNCH_CK();
-            off2 += K[i];
+            items = sorted;
         }
-        radix_sort<uint32_t, uint32_t>(c, ikey, ival, nitems, nullptr, 0, 16, (c.bpfx + "b.isort").c_str());
-        k_permute_items<<<grid_for(nitems, 128), 128, 0, c.stream>>>(items, ival, nitems, sorted);
-        FGSS_LAUNCH_CK();
-        items = sorted;
     }
-    // result buffers: the caller's size, the learned estimate (x1.5 + slack),
-    // or the last size seen for this slot
-    JoinArgs* d_args = c.devT<JoinArgs>(c.bpfx + "b.args", nj);
-    JoinArgs* hargs = c.pinnedT<JoinArgs>(c.bpfx + "b.hargs", nj);
-    for (size_t i = 0; i < nj; i++) {
-        JoinState& J = *joins[i];
-        const uint64_t n = J.in.n_sets;
-        uint64_t cap;
-        if (capture) {
-            cap = plan->res_cap[i];
-        } else {
-            auto itc = c.tune.find(J.pfx("rescap"));
-            const uint64_t last = itc != c.tune.end() ? (uint64_t)itc->second.ctas_per_sm : 0;
-            if (J.res_cap_hint) {
-                cap = J.res_cap_hint;
-            } else if (J.res_cap_user) {
-                cap = J.res_cap_user;
-            } else if (use_model && c.model) {
-                // predicted results x 1.5 + slack, or the size this slot needed last time if larger
-                cap = std::max<uint64_t>((uint64_t)((double)htot[nj + i] * 1.5) + 4096, last);
-            } else {
-                cap = std::max<uint64_t>(n + 4096, last);
-            }
-            cap = std::min<uint64_t>(cap, 0xfffffff0ull);
-        }
-        JoinArgs& a = J.args;
-        a.res_cap = (uint32_t)cap;
-        a.heavy_min_qp = te.heavy_min_probe > 0 ? (uint32_t)te.heavy_min_probe : 0xffffffffu;
-        a.res_q = c.devT<uint32_t>(J.pfx("res.q"), cap + 1);
-        a.res_s = c.devT<uint32_t>(J.pfx("res.s"), cap + 1);
-        a.res_o = c.devT<uint32_t>(J.pfx("res.o"), cap + 1);
-        a.res_count = J.status + 3;
-        FGSS_CK(cudaMemsetAsync(a.heavy_count, 0, 8, c.stream));  // heavy_count + res_count
-        hargs[i] = a;
-    }
-    FGSS_CK(cudaMemcpyAsync(d_args, hargs, nj * sizeof(JoinArgs), cudaMemcpyHostToDevice, c.stream));
-    uint32_t* counter = c.devT<uint32_t>(c.bpfx + "b.counter", 4 + nj);
-    FGSS_CK(cudaMemsetAsync(counter, 0, (4 + nj) * 4, c.stream));
-    // (inside a capture the events must be external record nodes to be timed at replay)
-    const unsigned rec_flags = capture ? cudaEventRecordExternal : 0u;
-    FGSS_CK(cudaEventRecordWithFlags(c.ev[4], c.stream, rec_flags));
+
     bool sided = false;
     for (size_t i = 0; i < nj; i++) sided |= joins[i]->args.side != nullptr;
-    if (nitems) fused_launch(c, te, d_args, d_fargs, items, (uint32_t)nitems, counter, sided);
-    FGSS_CK(cudaEventRecordWithFlags(c.ev[5], c.stream, rec_flags));
-    c.probe_timed = true;
-    // heavy queries: one persistent launch per join.  Eagerly only when some
-    // were queued; under a plan always, with scratch for a fixed slot count
-    // (a launch with an empty queue returns at once).
-    uint32_t* hbuf = c.pinnedT<uint32_t>(c.bpfx + "b.hq", 2 * nj + 2);
-    if (!capture) {
-        for (size_t i = 0; i < nj; i++)
-            FGSS_CK(cudaMemcpyAsync(hbuf + 2 * i, joins[i]->status + 2, 8, cudaMemcpyDeviceToHost, c.stream));
-        c.sync();
-    }
-    for (size_t i = 0; i < nj; i++) {
-        JoinState& J = *joins[i];
-        uint32_t slots;
-        if (capture) {
-            slots = plan->heavy_slots[i];
-        } else {
-            const uint32_t nh = hbuf[2 * i];
-            slots = plan ? std::min<uint32_t>((uint32_t)std::max<uint64_t>(J.in.n_sets, 1), (uint32_t)c.num_sms)
-                         : std::min<uint32_t>(nh, (uint32_t)c.num_sms);
-            if (!nh && !plan) slots = 0;
+    uint32_t* counter = c.devT<uint32_t>(p + "b.counter", 4 + nj);
+    uint32_t* hst = c.pinnedT<uint32_t>(p + "b.hst", nj * 8);
+    std::vector<uint64_t> cap(nj, 0);
+    uint32_t slots = 0;
+    // (inside a capture the events must be external record nodes to be timed at replay)
+    const unsigned rec_flags = capture ? cudaEventRecordExternal : 0u;
+    for (int attempt = 0;; attempt++) {
+        // result buffers: the caller's size, the learned estimate (x1.5 +
+        // slack), the last size seen for this slot, or the exact count after
+        // an overflow
+        std::vector<uint64_t> capoff(nj + 1, 0);
+        for (size_t i = 0; i < nj; i++) {
+            JoinState& J = *joins[i];
+            if (capture) {
+                cap[i] = plan->res_cap[i];
+            } else {
+                auto itc = c.tune.find(J.pfx("rescap"));
+                const uint64_t last = itc != c.tune.end() ? (uint64_t)itc->second.ctas_per_sm : 0;
+                uint64_t v;
+                if (J.res_cap_hint) v = J.res_cap_hint;
+                else if (J.res_cap_user) v = J.res_cap_user;
+                else if (model) v = std::max<uint64_t>((uint64_t)((double)hsum[nj + i] * 1.5) + 4096, last);
+                else v = std::max<uint64_t>(J.in.n_sets + 4096, last);
+                cap[i] = std::min<uint64_t>(v, 0xfffffff0ull);
+            }
+            capoff[i + 1] = capoff[i] + cap[i];
         }
-        if (!slots) continue;
-        const HeavyScratch hs = heavy_scratch(c, c.bpfx, J.in.n_sets, slots, capture);
-        k_probe_heavy<MODE_FUSED, 512><<<slots, 512, 0, c.stream>>>(d_args, (uint32_t)i, hs.zero, hs.zero_words, hs.aux,
-                                                                    hs.aux_words, counter + 4 + i);
+        uint32_t* res_q = c.devT<uint32_t>(p + "b.res.q", capoff[nj] + 1);
+        uint32_t* res_s = c.devT<uint32_t>(p + "b.res.s", capoff[nj] + 1);
+        uint32_t* res_o = c.devT<uint32_t>(p + "b.res.o", capoff[nj] + 1);
+        for (size_t i = 0; i < nj; i++) {
+            JoinArgs& a = joins[i]->args;
+            a.res_cap = (uint32_t)cap[i];
+            a.heavy_min_qp = te.heavy_min_probe > 0 ? (uint32_t)te.heavy_min_probe : 0xffffffffu;
+            a.res_q = res_q + capoff[i];
+            a.res_s = res_s + capoff[i];
+            a.res_o = res_o + capoff[i];
+        }
+        upload_args(c, B, p + "b.ha2");
+        FGSS_CK(cudaMemsetAsync(counter, 0, (4 + nj) * 4, c.stream));
+        FGSS_CK(cudaEventRecordWithFlags(c.ev[4], c.stream, rec_flags));
+        if (nitems) fused_launch(c, te, B.d_args, pp.d_fargs, items, (uint32_t)nitems, counter, sided);
+        FGSS_CK(cudaEventRecordWithFlags(c.ev[5], c.stream, rec_flags));
+        c.probe_timed = true;
+        // queries deferred to the global-memory accumulator: one persistent
+        // launch for every join.  Eagerly only when some were queued; under a
+        // plan always, with scratch for a fixed slot count (a launch whose
+        // queues are empty returns at once).
+        uint32_t max_nh = 0;
+        if (!capture) {
+            FGSS_CK(cudaMemcpyAsync(hst, B.status, nj * 32, cudaMemcpyDeviceToHost, c.stream));
+            c.sync();
+            for (size_t i = 0; i < nj; i++) max_nh = std::max(max_nh, hst[8 * i + 2]);
+        }
+        const uint32_t all_slots = std::min<uint32_t>(std::max<uint32_t>(B.n_max, 1), (uint32_t)c.num_sms);
+        slots = capture ? plan->heavy_slots : plan ? all_slots : std::min<uint32_t>(max_nh, (uint32_t)c.num_sms);
+        if (slots) {
+            const HeavyScratch hs = heavy_scratch(c, p, B.n_max, slots, capture);
+            k_probe_heavy<MODE_FUSED, 512><<<slots, 512, 0, c.stream>>>(B.d_args, 0, (uint32_t)nj, hs.zero,
+                                                                        hs.zero_words, hs.aux, hs.aux_words,
+                                                                        counter + 4);
+            FGSS_LAUNCH_CK();
+        }
+        if (capture) break;
+        FGSS_CK(cudaMemcpyAsync(hst, B.status, nj * 32, cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+        bool over = false;
+        for (size_t i = 0; i < nj; i++) {
+            JoinState& J = *joins[i];
+            const uint32_t got = hst[8 * i + 3];
+            if (got > cap[i]) {
+                // The learned (or remembered) capacity was too small: the kernel
+                // kept counting, so the batch re-runs with the exact size.  A
+                // plan keeps that exact size for the captured batch.
+                J.res_cap_hint = got;
+                J.overflow_retries++;
+                over = true;
+            }
+        }
+        if (!over) break;
+        if (attempt) fail(FGSS_ERR_CUDA, "result buffers overflowed at their exact size");
+        k_clear_filter_state_mj<<<(unsigned)std::min<size_t>(nj, 1024), 32, 0, c.stream>>>(B.d_args, (uint32_t)nj);
         FGSS_LAUNCH_CK();
     }
     if (plan && !capture) {
         plan->te = te;
         plan->K = K;
         plan->nitems = nitems;
-        plan->heavy_slots.assign(nj, 0);
-        for (size_t i = 0; i < nj; i++)
-            plan->heavy_slots[i] =
-                std::min<uint32_t>((uint32_t)std::max<uint64_t>(joins[i]->in.n_sets, 1), (uint32_t)c.num_sms);
-        plan->res_cap.assign(nj, 0);
+        plan->heavy_slots = slots;
+        plan->res_cap = cap;
     }
-    if (capture) {
-        // results sorted at full capacity; the host reads the counts after replay
-        for (size_t i = 0; i < nj; i++) {
-            JoinState& J = *joins[i];
-            uint64_t* keys = c.devT<uint64_t>(J.pfx("rkey"), (uint64_t)J.args.res_cap + 1);
-            uint32_t* vals = c.devT<uint32_t>(J.pfx("rval"), (uint64_t)J.args.res_cap + 1);
-            J.d_nres = c.devT<uint64_t>(J.pfx("nres"), 2);
-            k_result_keys<<<grid_for(J.args.res_cap, 256, c.num_sms * 32), 256, 0, c.stream>>>(
-                J.args.res_q, J.args.res_s, J.args.res_o, J.status + 3, J.args.res_cap, keys, vals, J.d_nres);
-            FGSS_LAUNCH_CK();
-            join_output(c, J, keys, vals, J.d_nres, J.args.res_cap);
-        }
-        return;
-    }
-    // results: overflow -> exact re-run of that join with the exact capacity
-    for (size_t i = 0; i < nj; i++)
-        FGSS_CK(cudaMemcpyAsync(hbuf + 2 * i, joins[i]->status + 3, 4, cudaMemcpyDeviceToHost, c.stream));
-    c.sync();
-    const std::vector<uint32_t> gots = [&] {
-        std::vector<uint32_t> g(nj);
-        for (size_t i = 0; i < nj; i++) g[i] = hbuf[2 * i];
-        return g;
-    }();
+
+    // results: join j's in the output columns from out_off[j] (its result
+    // count eagerly, its capacity under a plan, so a captured graph finds
+    // every buffer at the size it has now)
+    std::vector<uint64_t> rcap(nj);
     for (size_t i = 0; i < nj; i++) {
         JoinState& J = *joins[i];
-        const uint32_t got = gots[i];
-        if (got > J.args.res_cap) {
-            // The learned (or remembered) capacity was too small: the kernel kept
-            // counting, so re-run this join alone with the exact size.  A plan
-            // keeps that exact size for the captured batch.
-            J.res_cap_hint = got;
-            J.overflow_retries++;
-            k_clear_filter_state<<<1, 32, 0, c.stream>>>(J.status, J.stats);
-            FGSS_LAUNCH_CK();
-            std::vector<JoinState*> one{&J};
-            batched_filter_verify(c, one, false, nullptr);
-            if (plan) plan->res_cap[i] = J.args.res_cap;
+        if (capture) {
+            rcap[i] = cap[i];
             continue;
         }
-        if (plan) plan->res_cap[i] = J.args.res_cap;
-        // remember a sufficient capacity for the next call on this slot
-        J.res_cap_hint = 0;
-        c.tune[J.pfx("rescap")].ctas_per_sm = (int)std::min<uint64_t>((uint64_t)got + got / 4 + 1024, 0x7fffffff);
-        uint64_t* keys = c.devT<uint64_t>(J.pfx("rkey"), (uint64_t)J.args.res_cap + 1);
-        uint32_t* vals = c.devT<uint32_t>(J.pfx("rval"), (uint64_t)J.args.res_cap + 1);
-        J.d_nres = c.devT<uint64_t>(J.pfx("nres"), 2);
-        if (got) {
-            k_result_keys<<<grid_for(got, 256, c.num_sms * 32), 256, 0, c.stream>>>(
-                J.args.res_q, J.args.res_s, J.args.res_o, J.status + 3, J.args.res_cap, keys, vals, J.d_nres);
-            FGSS_LAUNCH_CK();
-        } else {
-            FGSS_CK(cudaMemsetAsync(J.d_nres, 0, 8, c.stream));
-        }
-        // under a plan, the output stage is sized at capacity so the captured
-        // graph finds every buffer at the size it has now
-        join_output(c, J, keys, vals, J.d_nres, plan ? (uint64_t)J.args.res_cap : (uint64_t)got);
+        const uint32_t got = hst[8 * i + 3];
         J.n_res = got;
+        J.res_cap_hint = 0;
+        // remember a sufficient capacity for the next call on this slot
+        c.tune[J.pfx("rescap")].ctas_per_sm = (int)std::min<uint64_t>((uint64_t)got + got / 4 + 1024, 0x7fffffff);
+        rcap[i] = plan ? cap[i] : got;
+    }
+    B.out_off.assign(nj + 1, 0);
+    for (size_t i = 0; i < nj; i++) B.out_off[i + 1] = B.out_off[i] + rcap[i];
+    B.out_cap = B.out_off[nj];
+    const uint64_t oc = B.out_cap;
+    B.oq = c.devT<uint32_t>(p + "b.o.q", oc + 1);
+    B.os = c.devT<uint32_t>(p + "b.o.s", oc + 1);
+    B.oidq = c.devT<uint32_t>(p + "b.o.idq", oc + 1);
+    B.oids = c.devT<uint32_t>(p + "b.o.ids", oc + 1);
+    B.oo = c.devT<uint32_t>(p + "b.o.o", oc + 1);
+    B.osim = c.devT<float>(p + "b.o.sim", oc + 1);
+    for (size_t i = 0; i < nj; i++) {
+        JoinState& J = *joins[i];
+        const uint64_t o = B.out_off[i];
+        J.oq = B.oq + o;
+        J.os = B.os + o;
+        J.oidq = B.oidq + o;
+        J.oids = B.oids + o;
+        J.oo = B.oo + o;
+        J.osim = B.osim + o;
+    }
+    if (oc == 0) return;
+    const TileMap rt = upload_tiles(c, p + "b.rt", B.out_off, 256);
+    uint64_t* resoff = c.devT<uint64_t>(p + "b.resoff", nj + 2);
+    uint64_t* d_n = resoff + nj + 1;
+    k_result_offsets<<<1, 1024, 0, c.stream>>>(B.d_args, (uint32_t)nj, resoff, d_n);
+    FGSS_LAUNCH_CK();
+    // sort keys join << 2qb | q << qb | s: only the bits that vary
+    const int qb = bits_for(B.n_max), jb = bits_for(nj);
+    if (2 * qb + jb > 64) fail(FGSS_ERR_UNSUPPORTED, "result keys of more than 64 bits");
+    uint64_t* key = c.devT<uint64_t>(p + "b.rkey", oc + 1);
+    uint32_t* val = c.devT<uint32_t>(p + "b.rval", oc + 1);
+    k_result_keys_mj<<<tile_grid(c, rt), 256, 0, c.stream>>>(B.d_args, rt, resoff, (uint32_t)qb, key, val);
+    FGSS_LAUNCH_CK();
+    radix_sort<uint64_t, uint32_t>(c, key, val, oc, d_n, 0, 2 * qb + jb, (p + "b.rsort").c_str());
+    k_result_out_mj<<<grid_for(oc, 256, c.num_sms * 32), 256, 0, c.stream>>>(
+        B.d_args, key, val, d_n, resoff, rt.roff, (uint32_t)qb, B.oq, B.os, B.oidq, B.oids, B.oo, B.osim);
+    FGSS_LAUNCH_CK();
+}
+
+void batch_finish_status(Ctx& c, Batch& B) {
+    const size_t nj = B.js.size();
+    uint32_t* h = c.pinnedT<uint32_t>(c.bpfx + "b.hfin", nj * 8);
+    unsigned long long* hs = c.pinnedT<unsigned long long>(c.bpfx + "b.hfin.stats", nj * SS_N);
+    uint64_t* he = c.pinnedT<uint64_t>(c.bpfx + "b.hfin.E", nj * 2);
+    FGSS_CK(cudaMemcpyAsync(h, B.status, nj * 32, cudaMemcpyDeviceToHost, c.stream));
+    FGSS_CK(cudaMemcpyAsync(hs, B.stats, nj * SS_N * 8, cudaMemcpyDeviceToHost, c.stream));
+    FGSS_CK(cudaMemcpyAsync(he, B.d_e, nj * 16, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    for (size_t j = 0; j < nj; j++) {
+        B.js[j]->n_entries = he[2 * j];
+        B.js[j]->n_res = h[8 * j + 3];
+        apply_status(*B.js[j], h[8 * j], hs + SS_N * j);
     }
 }
 

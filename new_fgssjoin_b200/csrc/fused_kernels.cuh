@@ -28,7 +28,7 @@ namespace fgss {
 // number of prefix matches (10).
 constexpr uint32_t kSmaxUnknown = 2047;
 
-// Layout: slots u64[H] | occ u16[H] | sls u16[H] | wlo,whi,clo u32[PC] |
+// Layout: slots u64[H] | occ u16[H] | sls u16[H] | clo u32[PC] |
 //         wpre u32[PC+4] | qtok u32[QC] | bm u32[BW] | mlist u16[MC]
 template <int HLOG>
 struct FusedLayout {
@@ -36,16 +36,14 @@ struct FusedLayout {
     static constexpr uint32_t cap = H / 2;    // window entries per chunk
     // probe tokens handled in shared memory: 256..512 (a slot's 11-bit query
     // position and 10-bit match count rely on PC <= 512)
-    static constexpr uint32_t PC = H / 4 > 512 ? 512 : (H / 4 > 256 ? H / 4 : 256);
-    static constexpr uint32_t QC = H / 2 > 1024 ? 1024 : H / 2;  // query tokens staged in shared memory
+    static constexpr uint32_t PC = H / 4 > 384 ? 384 : (H / 4 > 256 ? H / 4 : 256);
+    static constexpr uint32_t QC = H / 2 > 512 ? 512 : H / 2;  // query tokens staged in shared memory
                                                                   // (longer: read from HBM)
     static constexpr uint32_t BW = 1024;      // bitmap words: 32768 bits
-    static constexpr uint32_t MC = 512;       // merge list entries per chunk (more: merged by their lane)
+    static constexpr uint32_t MC = 256;       // merge list entries per chunk (more: merged by their lane)
     static constexpr size_t off_occ = 8ull * H;
     static constexpr size_t off_sls = off_occ + 2ull * H;   // source size of each slot
-    static constexpr size_t off_wlo = off_sls + 2ull * H;
-    static constexpr size_t off_whi = off_wlo + 4ull * PC;
-    static constexpr size_t off_clo = off_whi + 4ull * PC;
+    static constexpr size_t off_clo = off_sls + 2ull * H;
     static constexpr size_t off_wpre = off_clo + 4ull * PC;
     static constexpr size_t off_qtok = off_wpre + 4ull * (PC + 4);
     static constexpr size_t off_bm = off_qtok + 4ull * QC;
@@ -54,94 +52,88 @@ struct FusedLayout {
     static_assert(off_bm % 16 == 0, "the membership words are cleared with 16-byte stores");
 };
 
-// Window of every probe token: warp per query.  win[poff[q] + j] = (lo, hi),
-// wpre[poff[q] + j] = entries in the query's windows before window j,
+// Windows of one query's probe tokens (warp-collective): win[poff[q] + j] =
+// (lo, hi), wpre[poff[q] + j] = entries in the query's windows before window j,
 // wtot[q] = sum of the window sizes (also meta[q].w).
-static __global__ void k_windows(JoinArgs a, const uint32_t* __restrict__ poff, uint2* __restrict__ win,
-                                 uint32_t* __restrict__ wpre, uint32_t* __restrict__ wtot,
-                                 uint4* __restrict__ meta) {
-    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+__device__ __forceinline__ void windows_query(const JoinArgs& a, uint32_t q, const uint32_t* __restrict__ poff,
+                                              uint2* __restrict__ win, uint32_t* __restrict__ wpre,
+                                              uint32_t* __restrict__ wtot, uint4* __restrict__ meta) {
     const uint32_t lane = lane_id();
     const bool unsorted = (*a.status & ST_UNSORTED) != 0;
-    for (uint32_t q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < a.n; q += warps) {
-        const uint32_t lq = a.len[q];
-        const bool mine = q >= a.q_lo && q < a.q_hi;
-        const uint32_t qp = (lq <= 65535u && mine) ? a.probe[lq] : 0;
-        const uint32_t send = unsorted ? a.n : (lq <= 65535u ? a.send[lq] : 0);
-        const uint32_t* qt = a.tok + a.pos[q];
-        const uint32_t o = poff[q];
-        uint32_t tot = 0;  // running total of the windows before this round (same in every lane)
-        for (uint32_t j0 = 0; j0 < qp; j0 += 32) {
-            const uint32_t j = j0 + lane;
-            uint32_t lo = 0, hi = 0;
-            if (j < qp) {
-                const uint32_t w = __ldg(qt + j);
-                const uint32_t b = __ldg(a.list_off + w), e = __ldg(a.list_off + w + 1);
-                lo = e;
-                hi = e;
-                if (send > q + 1) {
-                    lo = lower_bound_u32(a.ent_s, b, e, q + 1);
-                    hi = unsorted ? e : lower_bound_u32(a.ent_s, lo, e, send);
-                }
+    const uint32_t lq = a.len[q];
+    const bool mine = q >= a.q_lo && q < a.q_hi;
+    const uint32_t qp = (lq <= 65535u && mine) ? a.probe[lq] : 0;
+    const uint32_t send = unsorted ? a.n : (lq <= 65535u ? a.send[lq] : 0);
+    const uint32_t* qt = a.tok + a.pos[q];
+    const uint32_t o = poff[q];
+    uint32_t tot = 0;  // running total of the windows before this round (same in every lane)
+    for (uint32_t j0 = 0; j0 < qp; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        uint32_t lo = 0, hi = 0;
+        if (j < qp) {
+            const uint32_t w = __ldg(qt + j);
+            const uint32_t b = __ldg(a.list_off + w), e = __ldg(a.list_off + w + 1);
+            lo = e;
+            hi = e;
+            if (send > q + 1) {
+                lo = lower_bound_u32(a.ent_s, b, e, q + 1);
+                hi = unsorted ? e : lower_bound_u32(a.ent_s, lo, e, send);
             }
-            const uint32_t incl = warp_incl_scan(hi - lo);
-            if (j < qp) {
-                win[o + j] = make_uint2(lo, hi);
-                wpre[o + j] = tot + incl - (hi - lo);
-            }
-            tot += __shfl_sync(kFull, incl, 31);
         }
-        if (lane == 0) {
-            wtot[q] = tot;
-            meta[q] = make_uint4(a.pos[q], lq, lq <= 65535u ? a.index[lq] : 0u, tot);
+        const uint32_t incl = warp_incl_scan(hi - lo);
+        if (j < qp) {
+            win[o + j] = make_uint2(lo, hi);
+            wpre[o + j] = tot + incl - (hi - lo);
         }
+        tot += __shfl_sync(kFull, incl, 31);
+    }
+    if (lane == 0) {
+        wtot[q] = tot;
+        meta[q] = make_uint4(a.pos[q], lq, lq <= 65535u ? a.index[lq] : 0u, tot);
     }
 }
 
-// Chunk boundaries of the queries whose windows hold more than `cap` entries:
-// the id window [q+1, send) is cut into nch equal id ranges (sized for 3/4 of
-// cap on average) and, for every inner boundary id b and probe token j, the
-// first entry of j's window at or after b is stored.  Warp per query; the
+// Chunk boundaries of one query whose windows hold more than `cap` entries
+// (warp-collective): the id window [q+1, send) is cut into nch equal id ranges
+// (sized for 3/4 of cap on average) and, for every inner boundary id b and
+// probe token j, the first entry of j's window at or after b is stored.  The
 // boundary buffer is carved with one atomic per query; a query that does not
 // fit keeps nch = 1 and the fused kernel bisects it instead.
-static __global__ void k_chunks(JoinArgs a, const uint32_t* __restrict__ poff, const uint2* __restrict__ win,
-                                const uint32_t* __restrict__ wtot, uint32_t cap, uint2* __restrict__ qchunk,
-                                uint32_t* __restrict__ cbuf, uint64_t cbuf_cap,
-                                unsigned long long* __restrict__ cbuf_used) {
-    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+__device__ __forceinline__ void chunks_query(const JoinArgs& a, uint32_t q, const uint32_t* __restrict__ poff,
+                                             const uint2* __restrict__ win, const uint32_t* __restrict__ wtot,
+                                             uint32_t cap, uint2* __restrict__ qchunk, uint32_t* __restrict__ cbuf,
+                                             uint64_t cbuf_cap, unsigned long long* __restrict__ cbuf_used) {
     const uint32_t lane = lane_id();
     const bool unsorted = (*a.status & ST_UNSORTED) != 0;
-    for (uint32_t q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < a.n; q += warps) {
-        const uint32_t L = wtot[q];
-        uint32_t nch = 1;
-        unsigned long long base = 0;
-        const uint32_t lq = a.len[q];
-        const uint32_t qp = lq <= 65535u ? a.probe[lq] : 0;
-        const uint32_t send = unsorted ? a.n : (lq <= 65535u ? a.send[lq] : 0);
-        if (L > cap && qp > 0 && send > q + 2) {
-            const uint32_t span = send - q - 1;
-            uint64_t want = ((uint64_t)L * 4 + 3ull * cap - 1) / (3ull * cap);
-            nch = (uint32_t)(want < span ? want : span);
-            if (lane == 0) {
-                const unsigned long long need = (unsigned long long)(nch - 1) * qp;
-                base = atomicAdd(cbuf_used, need);
-                if (base + need > cbuf_cap) nch = 1;
-            }
-            nch = __shfl_sync(kFull, nch, 0);
-            base = __shfl_sync(kFull, base, 0);
-            if (nch > 1) {
-                const uint2* w = win + poff[q];
-                const uint32_t inner = (nch - 1) * qp;
-                for (uint32_t f = lane; f < inner; f += 32) {
-                    const uint32_t i = f / qp + 1, j = f % qp;
-                    const uint32_t b = q + 1 + (uint32_t)(((uint64_t)span * i) / nch);
-                    const uint2 wj = w[j];
-                    cbuf[base + f] = lower_bound_u32(a.ent_s, wj.x, wj.y, b);
-                }
+    const uint32_t L = wtot[q];
+    uint32_t nch = 1;
+    unsigned long long base = 0;
+    const uint32_t lq = a.len[q];
+    const uint32_t qp = lq <= 65535u ? a.probe[lq] : 0;
+    const uint32_t send = unsorted ? a.n : (lq <= 65535u ? a.send[lq] : 0);
+    if (L > cap && qp > 0 && send > q + 2) {
+        const uint32_t span = send - q - 1;
+        const uint64_t want = ((uint64_t)L * 4 + 3ull * cap - 1) / (3ull * cap);
+        nch = (uint32_t)(want < span ? want : span);
+        if (lane == 0) {
+            const unsigned long long need = (unsigned long long)(nch - 1) * qp;
+            base = atomicAdd(cbuf_used, need);
+            if (base + need > cbuf_cap) nch = 1;
+        }
+        nch = __shfl_sync(kFull, nch, 0);
+        base = __shfl_sync(kFull, base, 0);
+        if (nch > 1) {
+            const uint2* w = win + poff[q];
+            const uint32_t inner = (nch - 1) * qp;
+            for (uint32_t f = lane; f < inner; f += 32) {
+                const uint32_t i = f / qp + 1, j = f % qp;
+                const uint32_t b = q + 1 + (uint32_t)(((uint64_t)span * i) / nch);
+                const uint2 wj = w[j];
+                cbuf[base + f] = lower_bound_u32(a.ent_s, wj.x, wj.y, b);
             }
         }
-        if (lane == 0) qchunk[q] = make_uint2((uint32_t)base, nch);
     }
+    if (lane == 0) qchunk[q] = make_uint2((uint32_t)base, nch);
 }
 
 struct FusedArgs {
@@ -288,8 +280,6 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem);
     uint16_t* occ = reinterpret_cast<uint16_t*>(smem + Lay::off_occ);
     uint16_t* sls = reinterpret_cast<uint16_t*>(smem + Lay::off_sls);
-    uint32_t* wlo = reinterpret_cast<uint32_t*>(smem + Lay::off_wlo);
-    uint32_t* whi = reinterpret_cast<uint32_t*>(smem + Lay::off_whi);
     uint32_t* clo = reinterpret_cast<uint32_t*>(smem + Lay::off_clo);
     uint32_t* wpre = reinterpret_cast<uint32_t*>(smem + Lay::off_wpre);
     uint32_t* qtok = reinterpret_cast<uint32_t*>(smem + Lay::off_qtok);
@@ -337,11 +327,8 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     const bool one_chunk = nch == 1 && qm.w <= Lay::cap;
     const uint32_t* qpre = fa.wpre + fa.poff[q];
     for (uint32_t j = tid; j < qp; j += NT) {
-        const uint2 w = qwin[j];
-        wlo[j] = w.x;
-        whi[j] = w.y;
         if (one_chunk) {
-            clo[j] = w.x;
+            clo[j] = qwin[j].x;
             wpre[j] = qpre[j];
         }
     }
@@ -398,11 +385,12 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                             if (j < qp) {
                                 uint32_t lo, hi;
                                 if (tag != 0xffffffffu) {
-                                    lo = tag == 0 ? wlo[j] : cb[(tag - 1) * qp + j];
-                                    hi = tag + 1 == nch ? whi[j] : cb[tag * qp + j];
+                                    lo = tag == 0 ? qwin[j].x : cb[(tag - 1) * qp + j];
+                                    hi = tag + 1 == nch ? qwin[j].y : cb[tag * qp + j];
                                 } else {
-                                    lo = lower_bound_u32(a.ent_s, wlo[j], whi[j], ra);
-                                    hi = lower_bound_u32(a.ent_s, lo, whi[j], rb);
+                                    const uint2 wj = qwin[j];
+                                    lo = lower_bound_u32(a.ent_s, wj.x, wj.y, ra);
+                                    hi = lower_bound_u32(a.ent_s, lo, wj.y, rb);
                                 }
                                 cnt = hi - lo;
                                 clo[j] = lo;

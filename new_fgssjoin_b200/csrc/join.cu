@@ -16,20 +16,12 @@ void upload(Ctx& c, T* dst, const std::vector<T>& v) {
     FGSS_CK(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c.stream));
 }
 
-__global__ void k_widen(const uint32_t* in, uint64_t* out) { *out = *in; }
-
 __global__ void k_sum_u32(const uint32_t* __restrict__ in, uint64_t n, unsigned long long* out) {
     unsigned long long s = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         s += in[i];
     s = warp_sum(s);
     if (lane_id() == 0 && s) atomicAdd(out, s);
-}
-
-int bits_for(uint64_t v) {  // bits needed to hold values < v
-    int b = 1;
-    while (b < 64 && (1ull << b) < v) b++;
-    return b;
 }
 
 template <int MODE, int NT, int HLOG>
@@ -43,6 +35,14 @@ void set_smem_attr() {
 }
 
 }  // namespace
+
+__global__ void k_widen(const uint32_t* in, uint64_t* out) { *out = *in; }
+
+int bits_for(uint64_t v) {
+    int b = 1;
+    while (b < 64 && (1ull << b) < v) b++;
+    return b;
+}
 
 DevBounds device_bounds(Ctx& c, float t, int mode) {
     uint32_t bits;
@@ -79,7 +79,7 @@ DevBounds device_bounds(Ctx& c, float t, int mode) {
     return d;
 }
 
-void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_opts& o, int slot, bool check) {
+void join_setup_host(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_opts& o, int slot) {
     J.slot = slot;
     J.t = o.threshold;
     J.res_cap_user = o.result_capacity;
@@ -111,15 +111,6 @@ void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_o
     }
     J.id = J.in.id;
     J.lut = device_bounds(c, J.t, J.bounds);
-    J.status = c.devT<uint32_t>(J.pfx("status"), 8);
-    J.stats = c.devT<unsigned long long>(J.pfx("stats"), SS_N);
-    J.maxlen = J.status + 1;
-    FGSS_CK(cudaMemsetAsync(J.status, 0, 32, c.stream));
-    FGSS_CK(cudaMemsetAsync(J.stats, 0, SS_N * 8, c.stream));
-    J.icnt = c.devT<uint32_t>(J.pfx("icnt"), n + 1);
-    J.pcnt = c.devT<uint32_t>(J.pfx("pcnt"), n + 1);
-    J.d_e = c.devT<uint64_t>(J.pfx("E"), 2);
-    uint32_t* send = c.devT<uint32_t>(J.pfx("send"), kMaxLen + 1);
 
     JoinArgs& a = J.args;
     memset(&a, 0, sizeof a);
@@ -129,8 +120,6 @@ void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_o
     a.n = (uint32_t)n;
     a.n_terms = v.n_terms;
     a.n_tokens = v.n_tokens;
-    a.status = J.status;
-    a.stats = J.stats;
     a.probe = J.lut.probe;
     a.index = J.lut.index;
     a.minsz = J.lut.minsz;
@@ -138,9 +127,10 @@ void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_o
     a.cand_min = J.lut.cand_min;
     a.inter_min = J.lut.inter_min;
     a.need = J.lut.need;
-    a.send = send;
-    a.heavy_q = c.devT<uint32_t>(J.pfx("heavy_q"), n + 1);
-    a.heavy_count = J.status + 2;
+    a.lmin = J.lut.lmin;
+    a.id = J.id;
+    a.thr = J.t;
+    a.side = J.side;
     a.heavy_cap = (uint32_t)n;
     a.join_id = (uint32_t)slot;
     a.heavy_min_qp = 0xffffffffu;  // set by the batched method's launch shape
@@ -153,6 +143,26 @@ void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_o
         a.q_hi = (uint32_t)n;
     }
     J.term_bits = bits_for((uint64_t)v.n_terms + 1);
+}
+
+void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_opts& o, int slot, bool check) {
+    join_setup_host(c, J, v, o, slot);
+    const uint64_t n = J.in.n_sets;
+    J.status = c.devT<uint32_t>(J.pfx("status"), 8);
+    J.stats = c.devT<unsigned long long>(J.pfx("stats"), SS_N);
+    J.maxlen = J.status + 1;
+    FGSS_CK(cudaMemsetAsync(J.status, 0, 32, c.stream));
+    FGSS_CK(cudaMemsetAsync(J.stats, 0, SS_N * 8, c.stream));
+    J.icnt = c.devT<uint32_t>(J.pfx("icnt"), n + 1);
+    J.pcnt = c.devT<uint32_t>(J.pfx("pcnt"), n + 1);
+    J.d_e = c.devT<uint64_t>(J.pfx("E"), 2);
+    uint32_t* send = c.devT<uint32_t>(J.pfx("send"), kMaxLen + 1);
+    JoinArgs& a = J.args;
+    a.status = J.status;
+    a.stats = J.stats;
+    a.send = send;
+    a.heavy_q = c.devT<uint32_t>(J.pfx("heavy_q"), n + 1);
+    a.heavy_count = J.status + 2;
     if (n == 0) return;
     k_prep<<<grid_for(n, 256, c.num_sms * 16), 256, 0, c.stream>>>(a, J.icnt, J.pcnt, J.maxlen, 1);
     FGSS_LAUNCH_CK();
@@ -168,7 +178,10 @@ void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_o
 
 void join_check_input(Ctx& c, JoinState& J) {
     if (J.in.n_sets == 0) return;
-    const uint32_t st = c.pinnedT<uint32_t>(J.pfx("h.prep"), 4)[0];
+    check_input_status(c.pinnedT<uint32_t>(J.pfx("h.prep"), 4)[0]);
+}
+
+void check_input_status(uint32_t st) {
     if (st & ST_BAD_OFFSETS) fail(FGSS_ERR_FORMAT, "a record's pos + len exceeds n_tokens");
     if (st & ST_TOO_LONG) fail(FGSS_ERR_UNSUPPORTED, "a record has more than 65535 tokens");
     if (st & ST_BAD_TOKENS)
@@ -211,8 +224,12 @@ void join_finish_status(Ctx& c, JoinState& J) {
     FGSS_CK(cudaMemcpyAsync(h, J.status, 16, cudaMemcpyDeviceToHost, c.stream));
     FGSS_CK(cudaMemcpyAsync(hs, J.stats, SS_N * 8, cudaMemcpyDeviceToHost, c.stream));
     c.sync();
-    J.status_host = h[0];
-    memcpy(J.stats_host, hs, sizeof(J.stats_host));
+    apply_status(J, h[0], hs);
+}
+
+void apply_status(JoinState& J, uint32_t st, const unsigned long long* stats) {
+    J.status_host = st;
+    memcpy(J.stats_host, stats, sizeof(J.stats_host));
     if (J.status_host & ST_TOO_LONG) fail(FGSS_ERR_UNSUPPORTED, "a record has more than 65535 tokens");
     if (J.status_host & ST_BAD_TOKENS)
         fail(FGSS_ERR_FORMAT, "tokens must be strictly ascending inside each record and below n_terms");
@@ -270,7 +287,7 @@ void join_plain_filter_verify(Ctx& c, JoinState& J, bool want_cand) {
     if (nheavy) {
         hs = heavy_scratch(c, "", n, hslots, false);
         FGSS_CK(cudaMemsetAsync(qctr, 0, 4, c.stream));
-        k_probe_heavy<MODE_COUNT, 512><<<hslots, 512, 0, c.stream>>>(J.d_args, 0, hs.zero, hs.zero_words, hs.aux,
+        k_probe_heavy<MODE_COUNT, 512><<<hslots, 512, 0, c.stream>>>(J.d_args, 0, 1, hs.zero, hs.zero_words, hs.aux,
                                                                      hs.aux_words, qctr);
         FGSS_LAUNCH_CK();
     }
@@ -294,7 +311,7 @@ void join_plain_filter_verify(Ctx& c, JoinState& J, bool want_cand) {
     FGSS_LAUNCH_CK();
     if (nheavy) {
         FGSS_CK(cudaMemsetAsync(qctr, 0, 4, c.stream));
-        k_probe_heavy<MODE_FILL, 512><<<hslots, 512, 0, c.stream>>>(J.d_args, 0, hs.zero, hs.zero_words, hs.aux,
+        k_probe_heavy<MODE_FILL, 512><<<hslots, 512, 0, c.stream>>>(J.d_args, 0, 1, hs.zero, hs.zero_words, hs.aux,
                                                                     hs.aux_words, qctr);
         FGSS_LAUNCH_CK();
     }

@@ -6,6 +6,7 @@
 #include "bounds.h"
 #include "ctx.h"
 #include "join_kernels.cuh"
+#include "tiles.cuh"
 
 namespace fgss {
 
@@ -25,6 +26,8 @@ DevBounds device_bounds(Ctx& c, float t, int mode);
 
 // Per-query features of the learned cost model (one row per record).
 constexpr int kFeat = 8;
+
+int bits_for(uint64_t v);  // bits needed to hold values < v (at least 1)
 
 // Everything one join keeps on the device between stages.
 struct JoinState {
@@ -49,6 +52,7 @@ struct JoinState {
     uint32_t *oq = nullptr, *os = nullptr, *oidq = nullptr, *oids = nullptr, *oo = nullptr;
     float* osim = nullptr;
     uint64_t n_res = 0;
+    uint64_t n_entries = ~0ull;  // index entries once read back (batched method)
     uint64_t res_cap_hint = 0;   // exact result count after an overflow
     uint64_t res_cap_user = 0;   // caller's result capacity (fgss_join_opts.result_capacity)
     uint32_t overflow_retries = 0;
@@ -58,6 +62,7 @@ struct JoinState {
     uint64_t pred_results = 0;        // the learned model's estimates (batched method, 0 without it)
     uint64_t pred_candidates = 0;
     uint64_t* d_cost = nullptr;       // batched pre-pass: per-query work estimates
+    const uint8_t* side = nullptr;    // R-S join: side byte of every record (JoinArgs.side)
     std::string ns;                   // buffer-name namespace ("" or a captured graph's own "g<id>.")
     std::string pfx(const char* name) const { return ns + "j" + std::to_string(slot) + "." + name; }
 };
@@ -81,7 +86,15 @@ void rs_output(Ctx& c, JoinState& J, const RsInput& u);
 // check=false the caller synchronizes the stream once for a whole batch and
 // then calls join_check_input for every join before any kernel reads tokens.
 void join_setup(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_opts& o, int slot, bool check = true);
+// The part of join_setup both methods share: options, the input's copy to the
+// device (host input), the bound tables and the JoinArgs fields that need no
+// per-join buffer.
+void join_setup_host(Ctx& c, JoinState& J, const fgss_sets_view& v, const fgss_join_opts& o, int slot);
 void join_check_input(Ctx& c, JoinState& J);
+void check_input_status(uint32_t st);  // throws on the input-validation bits
+// Host copies of a join's status word and counters; throws on bad input or a
+// filter-table overflow.
+void apply_status(JoinState& J, uint32_t st, const unsigned long long* stats);
 void join_index(Ctx& c, JoinState& J);
 void join_plain_filter_verify(Ctx& c, JoinState& J, bool want_cand);
 void join_features(Ctx& c, JoinState& J, float* d_feat);
@@ -98,19 +111,59 @@ struct HeavyScratch {
 };
 HeavyScratch heavy_scratch(Ctx& c, const std::string& prefix, uint64_t n, uint32_t slots, bool capture);
 
+// The batched method's batch: every join's per-record arrays are slices
+// [roff[j], roff[j+1]) of batch-level buffers and every stage is one launch
+// for the whole batch (tiles of one join per CTA, tiles.cuh).  Buffers are
+// named under the context's batch namespace (c.bpfx).
+struct Batch {
+    std::vector<JoinState*> js;
+    std::vector<uint64_t> roff;        // nj + 1: first record of each join
+    uint64_t R = 0;                    // records of the batch
+    uint64_t E = 0, P = 0;             // index entries, probe windows (read back by batch_prep)
+    uint32_t n_max = 0;                // records of the largest join
+    uint32_t terms_max = 0;
+    TileMap rec{};                     // tiles of 256 records (device arrays)
+    JoinArgs* d_args = nullptr;        // nj
+    uint32_t* status = nullptr;        // nj x 8 (ST_* bits, longest record, heavy count, result count)
+    unsigned long long* stats = nullptr;  // nj x SS_N
+    uint64_t* d_e = nullptr;           // nj x 2: index entries per join
+    uint32_t *icnt = nullptr, *pcnt = nullptr;  // R + 1: index / probe prefix per record
+    uint32_t *ioff = nullptr, *poff = nullptr;  // R + 1: their exclusive scans (totals at R)
+    uint32_t* send = nullptr;          // nj x 65537
+    uint32_t* heavy_q = nullptr;       // R + 1
+    // output columns (batch_filter_verify): join j's at out_off[j]
+    std::vector<uint64_t> out_off;
+    uint64_t out_cap = 0;
+    uint32_t *oq = nullptr, *os = nullptr, *oidq = nullptr, *oids = nullptr, *oo = nullptr;
+    float* osim = nullptr;
+};
+
 // Host-side decisions of one batched run, recorded eagerly and reused when the
 // same batch is captured into a CUDA graph (batch.cu).
 struct BatchPlan {
     bool capture = false;             // issue device work only, with these decisions
     TuneEntry te;
+    uint64_t E_cap = 0, P_cap = 0;    // index entries, probe windows the buffers hold
     std::vector<uint32_t> K;          // work items per join
     uint64_t nitems = 0;
     std::vector<uint64_t> res_cap;    // result slots per join
-    std::vector<uint32_t> heavy_slots;
+    uint32_t heavy_slots = 0;
 };
-void batched_filter_verify(Ctx& c, std::vector<JoinState*>& joins, bool use_model, BatchPlan* plan = nullptr);
-// Per-query work estimates of one join (its index built), copied to host `out` (n values).
-void join_query_costs(Ctx& c, JoinState& J, bool use_model, uint64_t* out);
+// Setup of every join (join_setup_host, with the slot each JoinState holds),
+// the batch's buffers, the per-record counts and input validation of the whole
+// batch (one launch each) and the index and probe totals, read back with one
+// wait; throws on bad input.  Runs eagerly: a captured graph starts after it.
+void batch_prep(Ctx& c, Batch& B, const std::vector<JoinState*>& js, const fgss_sets_view* views,
+                const fgss_join_opts* opts);
+// The inverted index of every join: one entry scatter, one sort by (join,
+// term), one list pass.  E_cap: entries the buffers hold (>= B.E).
+void batch_index(Ctx& c, Batch& B, uint64_t E_cap);
+void batched_filter_verify(Ctx& c, Batch& B, bool use_model, BatchPlan* plan = nullptr);
+// Status words and counters of every join to the host (one copy, one wait).
+void batch_finish_status(Ctx& c, Batch& B);
+// Per-query work estimates of a one-join batch (its index built), copied to
+// host `out` (n values).
+void batch_query_costs(Ctx& c, Batch& B, bool use_model, uint64_t* out);
 
 // Autotuner (tune.cu): workload class of a join, the shapes to try, the
 // cache file.

@@ -74,6 +74,9 @@ struct JoinArgs {
     const uint32_t* inter_min;
     const uint32_t* need;
     const uint32_t* send;      // per query length: end of the source id window (sorted input)
+    const uint32_t* lmin;      // per query length: smallest source size the size filter keeps
+    const uint32_t* id;        // record ids (null: the memory index)
+    float thr;                 // the join's threshold
     // inverted index
     const uint32_t* list_off;  // [n_terms + 1]
     const uint32_t* ent_s;     // source record of each entry, ascending within a list
@@ -173,42 +176,42 @@ __device__ __forceinline__ uint32_t warp_merge_count(const uint32_t* q, uint32_t
 // ------------------------------------------------------------- prefix stage
 
 // Per record: prefix lengths (data.cu:241-257), validation of the input
-// (sizes, order, tokens), the skip test of block.cu:121-130 for one tile.
-static __global__ void k_prep(JoinArgs a, uint32_t* __restrict__ icnt, uint32_t* __restrict__ pcnt, uint32_t* maxlen,
-                       int check_tokens) {
-    const uint32_t n = a.n;
-    uint32_t local_max = 0, bad = 0;
-    unsigned long long probe = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t l = a.len[i];
-        local_max = max(local_max, l);
-        if ((uint64_t)a.pos[i] + l > a.n_tokens) {
-            bad |= ST_BAD_OFFSETS;
-            icnt[i] = 0;
-            pcnt[i] = 0;
-            continue;
-        }
-        if (l > 65535u) {
-            bad |= ST_TOO_LONG;
-            icnt[i] = 0;
-            pcnt[i] = 0;
-            continue;
-        }
-        if (i + 1 < n && a.len[i + 1] > l) bad |= ST_UNSORTED;
-        icnt[i] = a.index[l];
-        pcnt[i] = a.probe[l];
-        probe += a.probe[l];
-        if (check_tokens) {
-            const uint32_t* t = a.tok + a.pos[i];
-            uint32_t prev = 0;
-            for (uint32_t j = 0; j < l; j++) {
-                uint32_t v = t[j];
-                if (v >= a.n_terms || (j > 0 && v <= prev)) bad |= ST_BAD_TOKENS;
-                prev = v;
-            }
+// (sizes, order, tokens).  icnt / pcnt are the record's own slots.
+__device__ __forceinline__ void prep_record(const JoinArgs& a, uint32_t i, uint32_t* icnt, uint32_t* pcnt,
+                                            uint32_t& local_max, uint32_t& bad, unsigned long long& probe,
+                                            int check_tokens) {
+    const uint32_t l = a.len[i];
+    local_max = max(local_max, l);
+    if ((uint64_t)a.pos[i] + l > a.n_tokens) {
+        bad |= ST_BAD_OFFSETS;
+        *icnt = 0;
+        *pcnt = 0;
+        return;
+    }
+    if (l > 65535u) {
+        bad |= ST_TOO_LONG;
+        *icnt = 0;
+        *pcnt = 0;
+        return;
+    }
+    if (i + 1 < a.n && a.len[i + 1] > l) bad |= ST_UNSORTED;
+    *icnt = a.index[l];
+    *pcnt = a.probe[l];
+    probe += a.probe[l];
+    if (check_tokens) {
+        const uint32_t* t = a.tok + a.pos[i];
+        uint32_t prev = 0;
+        for (uint32_t j = 0; j < l; j++) {
+            const uint32_t v = t[j];
+            if (v >= a.n_terms || (j > 0 && v <= prev)) bad |= ST_BAD_TOKENS;
+            prev = v;
         }
     }
-    // block reduce of max / flags
+}
+
+// Warp-collective: the warp's maximum size, status bits and probe-token count to the join.
+__device__ __forceinline__ void prep_flush(const JoinArgs& a, uint32_t* maxlen, uint32_t local_max, uint32_t bad,
+                                           unsigned long long probe) {
     local_max = __reduce_max_sync(kFull, local_max);
     bad = __reduce_or_sync(kFull, bad);
     probe = warp_sum(probe);
@@ -217,46 +220,65 @@ static __global__ void k_prep(JoinArgs a, uint32_t* __restrict__ icnt, uint32_t*
         if (bad) atomicOr(a.status, bad);
         if (probe) atomicAdd(&a.stats[SS_PROBE], probe);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0 && n > 0) {
-        // one-tile skip test (block.cu:121-123) -- only reachable for unsorted input
-        uint32_t l0 = a.len[0], ln = a.len[n - 1];
-        if (l0 <= 65535u && ln > a.maxsz[l0]) atomicOr(a.status, ST_SKIP_ALL);
-    }
+}
+
+// The one-tile skip test of block.cu:121-130 (only reachable for unsorted input).
+__device__ __forceinline__ void prep_skip_test(const JoinArgs& a) {
+    if (a.n == 0) return;
+    const uint32_t l0 = a.len[0], ln = a.len[a.n - 1];
+    if (l0 <= 65535u && ln > a.maxsz[l0]) atomicOr(a.status, ST_SKIP_ALL);
+}
+
+static __global__ void k_prep(JoinArgs a, uint32_t* __restrict__ icnt, uint32_t* __restrict__ pcnt, uint32_t* maxlen,
+                              int check_tokens) {
+    uint32_t local_max = 0, bad = 0;
+    unsigned long long probe = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
+        prep_record(a, i, icnt + i, pcnt + i, local_max, bad, probe, check_tokens);
+    prep_flush(a, maxlen, local_max, bad, probe);
+    if (blockIdx.x == 0 && threadIdx.x == 0) prep_skip_test(a);
 }
 
 // send[L] for every query length L: the number of records of size >= lmin[L]
 // (records have non-increasing sizes).
-static __global__ void k_send(const uint32_t* __restrict__ len, uint32_t n, const uint32_t* __restrict__ lmin,
-                       uint32_t* __restrict__ send, uint32_t nl) {
-    for (uint32_t L = blockIdx.x * blockDim.x + threadIdx.x; L < nl; L += gridDim.x * blockDim.x) {
-        uint32_t target = lmin[L];
-        uint32_t lo = 0, hi = n;  // first i with len[i] < target
-        while (lo < hi) {
-            uint32_t mid = (lo + hi) >> 1;
-            if (len[mid] >= target) lo = mid + 1;
-            else hi = mid;
-        }
-        send[L] = lo;
+__device__ __forceinline__ uint32_t send_of(const uint32_t* __restrict__ len, uint32_t n, uint32_t target) {
+    uint32_t lo = 0, hi = n;  // first i with len[i] < target
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (len[mid] >= target) lo = mid + 1;
+        else hi = mid;
     }
+    return lo;
+}
+
+static __global__ void k_send(const uint32_t* __restrict__ len, uint32_t n, const uint32_t* __restrict__ lmin,
+                              uint32_t* __restrict__ send, uint32_t nl) {
+    for (uint32_t L = blockIdx.x * blockDim.x + threadIdx.x; L < nl; L += gridDim.x * blockDim.x)
+        send[L] = send_of(len, n, lmin[L]);
 }
 
 // -------------------------------------------------------------- index stage
 
-// Index entries of every record's index prefix: key = term, value = record << 32 | size << 16 | position.
-static __global__ void k_index_entries(JoinArgs a, const uint32_t* __restrict__ ioff, uint32_t* __restrict__ key,
-                                uint64_t* __restrict__ val) {
-    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n; i += warps) {
-        uint32_t l = a.len[i];
-        if (l > 65535u) continue;
-        uint32_t ip = a.index[l];
-        const uint32_t* t = a.tok + a.pos[i];
-        uint32_t o = ioff[i];
-        for (uint32_t j = lane_id(); j < ip; j += 32) {
-            key[o + j] = t[j];
-            val[o + j] = ((uint64_t)i << 32) | (l << 16) | j;
-        }
+// Index entries of one record's index prefix (warp-collective), written from
+// position o: key = tag | term, value = record << 32 | size << 16 | position.
+template <typename K>
+__device__ __forceinline__ void index_entries_record(const JoinArgs& a, uint32_t i, uint64_t o, K tag,
+                                                     K* __restrict__ key, uint64_t* __restrict__ val) {
+    const uint32_t l = a.len[i];
+    if (l > 65535u) return;
+    const uint32_t ip = a.index[l];
+    const uint32_t* t = a.tok + a.pos[i];
+    for (uint32_t j = lane_id(); j < ip; j += 32) {
+        key[o + j] = tag | (K)t[j];
+        val[o + j] = ((uint64_t)i << 32) | (l << 16) | j;
     }
+}
+
+static __global__ void k_index_entries(JoinArgs a, const uint32_t* __restrict__ ioff, uint32_t* __restrict__ key,
+                                       uint64_t* __restrict__ val) {
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n; i += warps)
+        index_entries_record<uint32_t>(a, i, ioff[i], 0u, key, val);
 }
 
 // After the stable sort by term: list offsets (no atomics: the thread at each
@@ -710,142 +732,162 @@ __global__ void __launch_bounds__(NT) k_probe(const JoinArgs* __restrict__ joins
 // query clears the sources it touched), in a buffer of their own so that no
 // other array, whatever its layout for another join, ever dirties them;
 // `aux` holds the touched and verify lists and the query's windows.
+// Joins [join_id, join_id + n_join) one after another, each with its own
+// queue counter (queue_counter[j - join_id]); the scratch is sized for the
+// largest of them.  Each round of NT joins first lists, in join order, the
+// ones with deferred queries, so a batch of joins without any costs one pass.
 template <int MODE, int NT>
 __global__ void __launch_bounds__(NT) k_probe_heavy(const JoinArgs* __restrict__ joins, uint32_t join_id,
-                                                    uint32_t* __restrict__ zero, uint64_t zero_words,
+                                                    uint32_t n_join, uint32_t* __restrict__ zero, uint64_t zero_words,
                                                     uint32_t* __restrict__ aux, uint64_t aux_words,
                                                     uint32_t* queue_counter) {
-    const JoinArgs& a = joins[join_id];
-    const uint32_t n = a.n;
-    uint32_t* gcnt = zero + (uint64_t)blockIdx.x * zero_words;
-    uint32_t* gmp = gcnt + n;
-    uint32_t* base = aux + (uint64_t)blockIdx.x * aux_words;
-    uint32_t* gtouch = base;
-    uint32_t* gver = base + (uint64_t)n;
-    uint32_t* wlo = base + 2 * (uint64_t)n;
-    uint32_t* wpre = wlo + 65536;
     __shared__ uint32_t s_item, s_nt, s_nv, s_tot, s_nc;
     __shared__ uint32_t wsum[33];
-    const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    constexpr uint32_t NW = NT / 32;
-    CtaCounters ctr = {0, 0, 0, 0, 0, 0, 0};
-    const uint32_t nheavy = min(*a.heavy_count, a.heavy_cap);
-    const bool unsorted = (*a.status & ST_UNSORTED) != 0;
-    for (;;) {
-        if (tid == 0) {
-            s_item = atomicAdd(queue_counter, 1u);
-            s_nt = 0;
-            s_nv = 0;
-            s_nc = 0;
+    __shared__ uint32_t s_act[NT];
+    for (uint32_t round = 0; round < n_join; round += NT) {
+        __syncthreads();  // every thread is done with the previous round's list
+        uint32_t nact;
+        {
+            const uint32_t jr = round + threadIdx.x;
+            const uint32_t has = (jr < n_join && *joins[join_id + jr].heavy_count > 0) ? 1u : 0u;
+            const uint32_t at = block_excl_scan<uint32_t>(has, wsum, &nact);
+            if (has) s_act[at] = jr;
         }
         __syncthreads();
-        const uint32_t it = s_item;
-        if (it >= nheavy) break;
-        const uint32_t q = a.heavy_q[it];
-        const uint32_t lq = a.len[q];
-        const uint32_t* qt = a.tok + a.pos[q];
-        const uint32_t qp = a.probe[lq];
-        const uint32_t send = unsorted ? n : a.send[lq];
-        for (uint32_t j = tid; j < qp; j += NT) {
-            uint32_t w = __ldg(qt + j);
-            uint32_t b = __ldg(a.list_off + w), e = __ldg(a.list_off + w + 1);
-            uint32_t lo = lower_bound_u32(a.ent_s, b, e, q + 1);
-            uint32_t hi = unsorted ? e : lower_bound_u32(a.ent_s, lo, e, max(send, q + 1));
-            wlo[j] = lo;
-            wpre[j] = hi - lo;
-        }
-        __syncthreads();
-        uint32_t carry = 0;
-        for (uint32_t b0 = 0; b0 < qp; b0 += NT) {
-            uint32_t j = b0 + tid;
-            uint32_t x = j < qp ? wpre[j] : 0;
-            uint32_t tot;
-            uint32_t pre = block_excl_scan<uint32_t>(x, wsum, &tot);
-            if (j < qp) wpre[j] = pre + carry;
-            carry += tot;
-        }
-        if (tid == 0) {
-            wpre[qp] = carry;
-            s_tot = carry;
-        }
-        __syncthreads();
-        const uint32_t L = s_tot;
-        if (tid == 0) {
-            ctr.window += L;
-            ctr.heavy++;
-        }
-        for (uint32_t f = tid; f < L; f += NT) {
-            uint32_t j = upper_bound_gen(wpre, 0, qp, f) - 1;
-            uint32_t k = wlo[j] + (f - wpre[j]);
-            uint32_t s = __ldg(a.ent_s + k);
-            uint32_t sp = __ldg(a.ent_pl + k) & 0xffffu;
-            if (unsorted && !size_ok(a, lq, a.len[s])) continue;
-            if (a.side && __ldg(a.side + s) == __ldg(a.side + q)) continue;
-            uint32_t old = atomicAdd(&gcnt[s], 1u);
-            if (old == 0) gtouch[atomicAdd(&s_nt, 1u)] = s;
-            atomicMax(&gmp[s], (j << 16) | sp);
-        }
-        __syncthreads();
-        const uint32_t nt = s_nt;
-        uint32_t my_cand = 0;
-        for (uint32_t i = tid; i < nt; i += NT) {
-            uint32_t s = gtouch[i];
-            uint32_t c = gcnt[s], m = gmp[s];
-            uint32_t jm = m >> 16, smx = m & 0xffffu;
-            uint32_t ls = a.len[s], S = lq + ls;
-            uint32_t ub1 = c + min(lq - jm, ls - smx);
-            if (ub1 >= a.cand_min[S]) my_cand++;
-            if (ub1 - 1 >= a.inter_min[S]) {
-                uint32_t v = atomicAdd(&s_nv, 1u);
-                if (MODE == MODE_FILL) {
-                    if (v < a.vcnt[q]) a.cand[a.voff[q] + v] = make_uint4(q, s, c, jm);
-                    else atomicOr(a.status, ST_HASH_FULL);
+        for (uint32_t x = 0; x < nact; x++) {
+            __syncthreads();  // every thread is done with the previous join's queue
+            const uint32_t jj = s_act[x];
+            const JoinArgs& a = joins[join_id + jj];
+            const uint32_t n = a.n;
+            uint32_t* gcnt = zero + (uint64_t)blockIdx.x * zero_words;
+            uint32_t* gmp = gcnt + n;
+            uint32_t* base = aux + (uint64_t)blockIdx.x * aux_words;
+            uint32_t* gtouch = base;
+            uint32_t* gver = base + (uint64_t)n;
+            uint32_t* wlo = base + 2 * (uint64_t)n;
+            uint32_t* wpre = wlo + 65536;
+            const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+            constexpr uint32_t NW = NT / 32;
+            CtaCounters ctr = {0, 0, 0, 0, 0, 0, 0};
+            const uint32_t nheavy = min(*a.heavy_count, a.heavy_cap);
+            const bool unsorted = (*a.status & ST_UNSORTED) != 0;
+            for (;;) {
+                if (tid == 0) {
+                    s_item = atomicAdd(queue_counter + jj, 1u);
+                    s_nt = 0;
+                    s_nv = 0;
+                    s_nc = 0;
                 }
-                else if (MODE == MODE_FUSED) gver[v] = s;
-            }
-        }
-        my_cand = warp_sum(my_cand);
-        if (lane == 0 && my_cand) atomicAdd(&s_nc, my_cand);
-        __syncthreads();
-        const uint32_t nv = s_nv;
-        if (MODE == MODE_COUNT) {
-            if (tid == 0) {
-                a.vcnt[q] = nv;
-                a.ccnt[q] = s_nc;
-                a.wcnt[q] = L;
-            }
-        } else if (MODE == MODE_FUSED) {
-            if (tid == 0) ctr.cand += s_nc;
-            for (uint32_t v = wid; v < nv; v += NW) {
-                uint32_t s = gver[v];
-                uint32_t c = gcnt[s], m = gmp[s];
-                uint32_t jm = m >> 16, smx = m & 0xffffu;
-                uint32_t ls = a.len[s], S = lq + ls;
-                uint32_t imin = a.inter_min[S];
-                uint32_t o = warp_merge_count(qt, jm + 1, lq, a.tok + a.pos[s], smx + 1, ls, c, imin);
-                if (lane == 0) {
-                    ctr.verified++;
-                    if (o >= imin && o > 0) {
-                        ctr.inter++;
-                        if (o >= a.need[S]) {
-                            ctr.res++;
-                            emit_result(a, q, s, o);
+                __syncthreads();
+                const uint32_t it = s_item;
+                if (it >= nheavy) break;
+                const uint32_t q = a.heavy_q[it];
+                const uint32_t lq = a.len[q];
+                const uint32_t* qt = a.tok + a.pos[q];
+                const uint32_t qp = a.probe[lq];
+                const uint32_t send = unsorted ? n : a.send[lq];
+                for (uint32_t j = tid; j < qp; j += NT) {
+                    uint32_t w = __ldg(qt + j);
+                    uint32_t b = __ldg(a.list_off + w), e = __ldg(a.list_off + w + 1);
+                    uint32_t lo = lower_bound_u32(a.ent_s, b, e, q + 1);
+                    uint32_t hi = unsorted ? e : lower_bound_u32(a.ent_s, lo, e, max(send, q + 1));
+                    wlo[j] = lo;
+                    wpre[j] = hi - lo;
+                }
+                __syncthreads();
+                uint32_t carry = 0;
+                for (uint32_t b0 = 0; b0 < qp; b0 += NT) {
+                    uint32_t j = b0 + tid;
+                    uint32_t x = j < qp ? wpre[j] : 0;
+                    uint32_t tot;
+                    uint32_t pre = block_excl_scan<uint32_t>(x, wsum, &tot);
+                    if (j < qp) wpre[j] = pre + carry;
+                    carry += tot;
+                }
+                if (tid == 0) {
+                    wpre[qp] = carry;
+                    s_tot = carry;
+                }
+                __syncthreads();
+                const uint32_t L = s_tot;
+                if (tid == 0) {
+                    ctr.window += L;
+                    ctr.heavy++;
+                }
+                for (uint32_t f = tid; f < L; f += NT) {
+                    uint32_t j = upper_bound_gen(wpre, 0, qp, f) - 1;
+                    uint32_t k = wlo[j] + (f - wpre[j]);
+                    uint32_t s = __ldg(a.ent_s + k);
+                    uint32_t sp = __ldg(a.ent_pl + k) & 0xffffu;
+                    if (unsorted && !size_ok(a, lq, a.len[s])) continue;
+                    if (a.side && __ldg(a.side + s) == __ldg(a.side + q)) continue;
+                    uint32_t old = atomicAdd(&gcnt[s], 1u);
+                    if (old == 0) gtouch[atomicAdd(&s_nt, 1u)] = s;
+                    atomicMax(&gmp[s], (j << 16) | sp);
+                }
+                __syncthreads();
+                const uint32_t nt = s_nt;
+                uint32_t my_cand = 0;
+                for (uint32_t i = tid; i < nt; i += NT) {
+                    uint32_t s = gtouch[i];
+                    uint32_t c = gcnt[s], m = gmp[s];
+                    uint32_t jm = m >> 16, smx = m & 0xffffu;
+                    uint32_t ls = a.len[s], S = lq + ls;
+                    uint32_t ub1 = c + min(lq - jm, ls - smx);
+                    if (ub1 >= a.cand_min[S]) my_cand++;
+                    if (ub1 - 1 >= a.inter_min[S]) {
+                        uint32_t v = atomicAdd(&s_nv, 1u);
+                        if (MODE == MODE_FILL) {
+                            if (v < a.vcnt[q]) a.cand[a.voff[q] + v] = make_uint4(q, s, c, jm);
+                            else atomicOr(a.status, ST_HASH_FULL);
+                        }
+                        else if (MODE == MODE_FUSED) gver[v] = s;
+                    }
+                }
+                my_cand = warp_sum(my_cand);
+                if (lane == 0 && my_cand) atomicAdd(&s_nc, my_cand);
+                __syncthreads();
+                const uint32_t nv = s_nv;
+                if (MODE == MODE_COUNT) {
+                    if (tid == 0) {
+                        a.vcnt[q] = nv;
+                        a.ccnt[q] = s_nc;
+                        a.wcnt[q] = L;
+                    }
+                } else if (MODE == MODE_FUSED) {
+                    if (tid == 0) ctr.cand += s_nc;
+                    for (uint32_t v = wid; v < nv; v += NW) {
+                        uint32_t s = gver[v];
+                        uint32_t c = gcnt[s], m = gmp[s];
+                        uint32_t jm = m >> 16, smx = m & 0xffffu;
+                        uint32_t ls = a.len[s], S = lq + ls;
+                        uint32_t imin = a.inter_min[S];
+                        uint32_t o = warp_merge_count(qt, jm + 1, lq, a.tok + a.pos[s], smx + 1, ls, c, imin);
+                        if (lane == 0) {
+                            ctr.verified++;
+                            if (o >= imin && o > 0) {
+                                ctr.inter++;
+                                if (o >= a.need[S]) {
+                                    ctr.res++;
+                                    emit_result(a, q, s, o);
+                                }
+                            }
                         }
                     }
                 }
+                __syncthreads();
+                for (uint32_t i = tid; i < nt; i += NT) {
+                    uint32_t s = gtouch[i];
+                    gcnt[s] = 0;
+                    gmp[s] = 0;
+                }
+                __syncthreads();
+            }
+            if (lane == 0) {
+                if (MODE == MODE_FUSED) flush_counters(a, ctr);
+                else if (MODE == MODE_COUNT && tid == 0 && ctr.heavy) atomicAdd(&a.stats[SS_HEAVY], ctr.heavy);
             }
         }
-        __syncthreads();
-        for (uint32_t i = tid; i < nt; i += NT) {
-            uint32_t s = gtouch[i];
-            gcnt[s] = 0;
-            gmp[s] = 0;
-        }
-        __syncthreads();
-    }
-    if (lane == 0) {
-        if (MODE == MODE_FUSED) flush_counters(a, ctr);
-        else if (MODE == MODE_COUNT && tid == 0 && ctr.heavy) atomicAdd(&a.stats[SS_HEAVY], ctr.heavy);
     }
 }
 
@@ -856,26 +898,30 @@ __global__ void __launch_bounds__(NT) k_probe_heavy(const JoinArgs* __restrict__
 // Warp per record (a long record's bitmap is nearly full and bounds little,
 // but it is exact, so the bound holds for every pair).  Width: bmw uint4 per
 // record, 2 (256 bits) or 4 (512 bits, for joins of longer records).
+// One record's bitmap (warp-collective); sw: the warp's 16 shared words.
+__device__ __forceinline__ void bitmap_record(const JoinArgs& a, uint32_t r, uint4* __restrict__ bmap, uint32_t bmw,
+                                              uint32_t* sw) {
+    const uint32_t lane = lane_id();
+    const uint32_t shift = bmw == 4 ? 23 : 24;  // bit index: top 9 or 8 bits of a multiplicative hash
+    if (lane < 16) sw[lane] = 0;
+    __syncwarp();
+    const uint32_t l = a.len[r];
+    const uint32_t* t = a.tok + a.pos[r];
+    for (uint32_t j = lane; j < l; j += 32) {
+        const uint32_t b = (__ldg(t + j) * 0x9E3779B1u) >> shift;
+        atomicOr(&sw[b >> 5], 1u << (b & 31));
+    }
+    __syncwarp();
+    if (lane < bmw)
+        bmap[(uint64_t)bmw * r + lane] = make_uint4(sw[4 * lane], sw[4 * lane + 1], sw[4 * lane + 2], sw[4 * lane + 3]);
+    __syncwarp();
+}
+
 static __global__ void k_bitmaps(JoinArgs a, uint4* __restrict__ bmap, uint32_t bmw) {
     __shared__ uint32_t sw[8][16];  // launched with 256 threads: a bitmap per warp
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t lane = lane_id(), wl = threadIdx.x >> 5;
-    const uint32_t shift = bmw == 4 ? 23 : 24;  // bit index: top 9 or 8 bits of a multiplicative hash
-    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < a.n; r += warps) {
-        if (lane < 16) sw[wl][lane] = 0;
-        __syncwarp();
-        const uint32_t l = a.len[r];
-        const uint32_t* t = a.tok + a.pos[r];
-        for (uint32_t j = lane; j < l; j += 32) {
-            const uint32_t b = (__ldg(t + j) * 0x9E3779B1u) >> shift;
-            atomicOr(&sw[wl][b >> 5], 1u << (b & 31));
-        }
-        __syncwarp();
-        if (lane < bmw)
-            bmap[bmw * r + lane] =
-                make_uint4(sw[wl][4 * lane], sw[wl][4 * lane + 1], sw[wl][4 * lane + 2], sw[wl][4 * lane + 3]);
-        __syncwarp();
-    }
+    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < a.n; r += warps)
+        bitmap_record(a, r, bmap, bmw, sw[threadIdx.x >> 5]);
 }
 
 // Bitmap width of a join in uint4 words: 4 (512 bits) when its records average

@@ -165,6 +165,57 @@ __global__ void __launch_bounds__(256) k_mlp_predict(const float* __restrict__ f
     }
 }
 
+// The same prediction for every join of a batch: rows are the batch's
+// records, one per thread of a tile (tiles.cuh; blockDim == tile), the sums
+// per join (one atomic per block each).
+__global__ void __launch_bounds__(256) k_mlp_predict_tiles(const float* __restrict__ feat, TileMap m,
+                                                           const float* __restrict__ Pg, uint32_t* __restrict__ pred,
+                                                           unsigned long long* res_sums,
+                                                           unsigned long long* cand_sums) {
+    __shared__ float P[kParamsAll];
+    __shared__ double s_rs[8];
+    __shared__ unsigned long long s_cs[8];
+    for (int i = threadIdx.x; i < kParamsAll; i += blockDim.x) P[i] = Pg[i];
+    __syncthreads();
+    const float calib = P[kParams + 1] > 0.f ? P[kParams + 1] : 1.f;
+    for (uint32_t b = blockIdx.x; b < m.ntiles; b += gridDim.x) {
+        const TileRange t = tile_range(m, b);
+        const uint64_t g = __ldg(m.roff + t.j) + t.r0 + threadIdx.x;
+        unsigned long long cs = 0;
+        double rs = 0.0;
+        if (t.r0 + threadIdx.x < t.r1) {
+            float x[kFeatM], hpre[kHidden], o[kOut];
+#pragma unroll
+            for (int f = 0; f < kFeatM; f++) x[f] = feat[g * kFeatM + f] * kInScale;
+            mlp_fwd(P, x, hpre, o);
+            const float ec = expf(fminf(fmaxf(o[0] * kOutScale, -kRateClamp), kRateClamp));
+            const float er = expf(fminf(fmaxf(o[1] * kOutScale, -kRateClamp), kRateClamp));
+            pred[g] = (uint32_t)fminf(ec + 0.5f, 1.0e9f);
+            cs = pred[g];
+            rs = (double)er;
+        }
+        rs = warp_sum(rs);
+        cs = warp_sum(cs);
+        if (lane_id() == 0) {
+            s_rs[threadIdx.x >> 5] = rs;
+            s_cs[threadIdx.x >> 5] = cs;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double r = 0.0;
+            unsigned long long c = 0;
+            for (uint32_t w = 0; w < (blockDim.x >> 5); w++) {
+                r += s_rs[w];
+                c += s_cs[w];
+            }
+            // expected results: summed per tile, then rounded up once
+            if (r > 0.0) atomicAdd(res_sums + t.j, (unsigned long long)ceil(r * (double)calib));
+            if (c) atomicAdd(cand_sums + t.j, c);
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void k_sum_cost(const uint32_t* __restrict__ c, uint64_t n, unsigned long long* out) {
     unsigned long long s = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -184,6 +235,15 @@ void model_predict(Ctx& c, const float* feat, uint64_t n, uint32_t* pred, uint64
     if (!c.model || !c.model->dev) fail(FGSS_ERR_INVALID, "no cost model loaded");
     k_mlp_predict<<<grid_for(n, 256, c.num_sms * 8), 256, 0, c.stream>>>(
         feat, n, c.model->dev, pred, (unsigned long long*)res_sum, (unsigned long long*)cand_sum);
+    FGSS_LAUNCH_CK();
+}
+
+void model_predict_tiles(Ctx& c, const float* feat, const TileMap& m, uint32_t* pred, uint64_t* res_sums,
+                         uint64_t* cand_sums) {
+    if (!c.model || !c.model->dev) fail(FGSS_ERR_INVALID, "no cost model loaded");
+    if (m.ntiles == 0) return;
+    k_mlp_predict_tiles<<<std::min<uint32_t>(m.ntiles, (uint32_t)c.num_sms * 8), 256, 0, c.stream>>>(
+        feat, m, c.model->dev, pred, (unsigned long long*)res_sums, (unsigned long long*)cand_sums);
     FGSS_LAUNCH_CK();
 }
 

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "ctx.h"
+#include "tiles.cuh"
 
 namespace fgss {
 
@@ -37,6 +38,10 @@ namespace fgss {
 // *cand_sum += sum of pred (when given)
 void model_predict(Ctx& c, const float* feat, uint64_t n, uint32_t* pred, uint64_t* res_sum,
                    uint64_t* cand_sum = nullptr);
+// The prediction for every join of a batch (tiles of 256 of its records):
+// res_sums[j] / cand_sums[j] += join j's sums.
+void model_predict_tiles(Ctx& c, const float* feat, const TileMap& m, uint32_t* pred, uint64_t* res_sums,
+                         uint64_t* cand_sums);
 // *out += sum of cost[0..n)
 void model_sum_cost(Ctx& c, const uint32_t* cost, uint64_t n, uint64_t* out);
 // Full-batch Adam training on (feat, target) rows already on the device;

@@ -15,7 +15,7 @@
 using namespace fgss;
 
 namespace fgss {
-__global__ void k_features(JoinArgs a, float t, float* __restrict__ feat, uint32_t* __restrict__ cost);
+__global__ void k_features(JoinArgs a, float* __restrict__ feat);
 }
 
 namespace {
@@ -63,14 +63,12 @@ fgss_status fgss_model_train(fgss_ctx* ctx, const fgss_sets_view* sets, const fl
             const uint64_t m = J.in.n_sets;
             if (!m) continue;
             uint32_t* rcnt = c.devT<uint32_t>("mt.rcnt", m + 1);
-            uint32_t* cost = c.devT<uint32_t>("mt.cost", m + 1);
             FGSS_CK(cudaMemsetAsync(rcnt, 0, m * 4, c.stream));
             if (J.n_res) {
                 k_res_hist<<<grid_for(J.n_res, 256, c.num_sms * 8), 256, 0, c.stream>>>(J.oq, J.n_res, rcnt);
                 FGSS_LAUNCH_CK();
             }
-            k_features<<<grid_for(m * 32, 256, c.num_sms * 32), 256, 0, c.stream>>>(J.args, J.t, feat + off * kFeat,
-                                                                                   cost);
+            k_features<<<grid_for(m * 32, 256, c.num_sms * 32), 256, 0, c.stream>>>(J.args, feat + off * kFeat);
             FGSS_LAUNCH_CK();
             k_targets<<<grid_for(m, 256, c.num_sms * 8), 256, 0, c.stream>>>(J.args.vcnt, rcnt, m, target + off * 2);
             FGSS_LAUNCH_CK();
