@@ -187,14 +187,17 @@ void index_sort(Ctx& c, Batch& B, uint64_t E_cap, int tbits, int jbits, const ui
     FGSS_LAUNCH_CK();
 }
 
-// The batch's pre-pass (index built): windows of every probe token (exact
-// per-query work), bitmaps, chunk splits for slot tables of cap_entries, the
-// learned model's estimates (model) and the work-item cost of every query
-// (window entries + 4 x predicted candidates + size) with its exclusive
-// prefix in cpre (total at cpre[R]).  d_sums: [0, nj) cost totals,
-// [nj, 2nj) predicted results, [2nj, 3nj) predicted candidates.
+// The batch's pre-pass, first part (index built): windows of every probe
+// token (exact per-query work), the learned model's estimates (model) and the
+// work-item cost of every query (window entries + 4 x predicted candidates +
+// size) with its exclusive prefix in cpre (total at cpre[R]).  d_sums:
+// [0, nj) cost totals, [nj, 2nj) predicted results, [2nj, 3nj) predicted
+// candidates, [3nj] chunk-boundary words for slot tables of cap_entries.
 struct Prepass {
-    FusedArgs* d_fargs = nullptr;
+    uint2* win = nullptr;
+    uint32_t* wpre = nullptr;
+    uint32_t* wtot = nullptr;
+    uint4* meta = nullptr;
     uint64_t* cost = nullptr;
     uint64_t* cpre = nullptr;
     uint64_t* d_sums = nullptr;
@@ -204,13 +207,45 @@ Prepass batch_prepass(Ctx& c, Batch& B, uint32_t cap_entries, uint64_t P_cap, bo
     const size_t nj = B.js.size();
     const std::string& p = c.bpfx;
     const uint64_t R = B.R;
-    uint2* win = c.devT<uint2>(p + "b.win", P_cap + 1);
-    uint32_t* wpre = c.devT<uint32_t>(p + "b.wpre", P_cap + 1);
-    uint32_t* wtot = c.devT<uint32_t>(p + "b.wtot", R + 1);
-    uint4* meta = c.devT<uint4>(p + "b.meta", R + 1);
+    Prepass pp;
+    pp.win = c.devT<uint2>(p + "b.win", P_cap + 1);
+    pp.wpre = c.devT<uint32_t>(p + "b.wpre", P_cap + 1);
+    pp.wtot = c.devT<uint32_t>(p + "b.wtot", R + 1);
+    pp.meta = c.devT<uint4>(p + "b.meta", R + 1);
+    float* feat = c.devT<float>(p + "b.feat", (R + 1) * kFeatures);
+    uint32_t* pred = c.devT<uint32_t>(p + "b.pred", R + 1);
+    pp.cost = c.devT<uint64_t>(p + "b.cost", R + 1);
+    pp.cpre = c.devT<uint64_t>(p + "b.cpre", R + 1);
+    pp.d_sums = c.devT<uint64_t>(p + "b.sums", 3 * nj + 2);
+    FGSS_CK(cudaMemsetAsync(pp.d_sums, 0, (3 * nj + 2) * 8, c.stream));
+    if (R == 0) return pp;
+    const unsigned g = tile_grid(c, B.rec);
+    k_windows_mj<<<g, 256, 0, c.stream>>>(B.d_args, B.rec, B.poff, pp.win, pp.wpre, pp.wtot, pp.meta);
+    FGSS_LAUNCH_CK();
+    if (model) {
+        k_features_mj<<<g, 256, 0, c.stream>>>(B.d_args, B.rec, feat);
+        FGSS_LAUNCH_CK();
+        model_predict_tiles(c, feat, B.rec, pred, pp.d_sums + nj, pp.d_sums + 2 * nj);
+    }
+    k_cost_mj<<<g, 256, 0, c.stream>>>(B.d_args, B.rec, pp.wtot, model ? pred : nullptr, cap_entries, pp.cost,
+                                       (unsigned long long*)(pp.d_sums + 3 * nj));
+    FGSS_LAUNCH_CK();
+    exclusive_scan<uint64_t>(c, pp.cost, pp.cpre, R, nullptr, pp.cpre + R, (p + "b.scan.c").c_str());
+    k_join_cost_totals<<<grid_for(nj, 128), 128, 0, c.stream>>>(B.rec.roff, (uint32_t)nj, pp.cpre, pp.d_sums);
+    FGSS_LAUNCH_CK();
+    return pp;
+}
+
+// Second part: every record's token bitmap and the chunk splits of the
+// queries whose windows exceed cap_entries, into a boundary buffer of
+// cbuf_cap words (a query that finds it full is bisected by the fused kernel
+// instead); returns the fused kernel's per-join arguments on the device.
+FusedArgs* batch_filters(Ctx& c, Batch& B, const Prepass& pp, uint32_t cap_entries, uint64_t cbuf_cap) {
+    const size_t nj = B.js.size();
+    const std::string& p = c.bpfx;
+    const uint64_t R = B.R;
     uint2* qchunk = c.devT<uint2>(p + "b.qchunk", R + 1);
-    const uint64_t cbuf_cap = 2 * P_cap + (1u << 20);  // overflowing queries bisect instead
-    uint32_t* cbuf = c.devT<uint32_t>(p + "b.cbuf", cbuf_cap);
+    uint32_t* cbuf = c.devT<uint32_t>(p + "b.cbuf", cbuf_cap + 1);
     std::vector<uint64_t> boff(nj + 1, 0);
     std::vector<uint32_t> bmw(nj);
     for (size_t j = 0; j < nj; j++) {
@@ -222,45 +257,26 @@ Prepass batch_prepass(Ctx& c, Batch& B, uint32_t cap_entries, uint64_t P_cap, bo
     for (size_t j = 0; j < nj; j++) {
         FusedArgs& f = hf[j];
         f.poff = B.poff + B.roff[j];
-        f.win = win;
-        f.wpre = wpre;
+        f.win = pp.win;
+        f.wpre = pp.wpre;
         f.smin = B.js[j]->lut.smin;
-        f.meta = meta + B.roff[j];
+        f.meta = pp.meta + B.roff[j];
         f.qchunk = qchunk + B.roff[j];
         f.cbuf = cbuf;
         f.bmap = bmap + boff[j];
         f.bmw = bmw[j];
     }
-    Prepass pp;
-    pp.d_fargs = c.devT<FusedArgs>(p + "b.fargs", nj);
-    FGSS_CK(cudaMemcpyAsync(pp.d_fargs, hf, nj * sizeof(FusedArgs), cudaMemcpyHostToDevice, c.stream));
+    FusedArgs* d_fargs = c.devT<FusedArgs>(p + "b.fargs", nj);
+    FGSS_CK(cudaMemcpyAsync(d_fargs, hf, nj * sizeof(FusedArgs), cudaMemcpyHostToDevice, c.stream));
     unsigned long long* cused = c.devT<unsigned long long>(p + "b.cused", 1);
     FGSS_CK(cudaMemsetAsync(cused, 0, 8, c.stream));
-    float* feat = c.devT<float>(p + "b.feat", (R + 1) * kFeatures);
-    uint32_t* pred = c.devT<uint32_t>(p + "b.pred", R + 1);
-    pp.cost = c.devT<uint64_t>(p + "b.cost", R + 1);
-    pp.cpre = c.devT<uint64_t>(p + "b.cpre", R + 1);
-    pp.d_sums = c.devT<uint64_t>(p + "b.sums", 3 * nj + 2);
-    FGSS_CK(cudaMemsetAsync(pp.d_sums, 0, (3 * nj + 2) * 8, c.stream));
-    if (R == 0) return pp;
+    if (R == 0) return d_fargs;
     const unsigned g = tile_grid(c, B.rec);
-    k_windows_mj<<<g, 256, 0, c.stream>>>(B.d_args, B.rec, B.poff, win, wpre, wtot, meta);
+    k_bitmaps_mj<<<g, 256, 0, c.stream>>>(B.d_args, d_fargs, B.rec);
     FGSS_LAUNCH_CK();
-    k_bitmaps_mj<<<g, 256, 0, c.stream>>>(B.d_args, pp.d_fargs, B.rec);
+    k_chunks_mj<<<g, 256, 0, c.stream>>>(B.d_args, d_fargs, B.rec, pp.wtot, cap_entries, cbuf, cbuf_cap, cused);
     FGSS_LAUNCH_CK();
-    k_chunks_mj<<<g, 256, 0, c.stream>>>(B.d_args, pp.d_fargs, B.rec, wtot, cap_entries, cbuf, cbuf_cap, cused);
-    FGSS_LAUNCH_CK();
-    if (model) {
-        k_features_mj<<<g, 256, 0, c.stream>>>(B.d_args, B.rec, feat);
-        FGSS_LAUNCH_CK();
-        model_predict_tiles(c, feat, B.rec, pred, pp.d_sums + nj, pp.d_sums + 2 * nj);
-    }
-    k_cost_mj<<<g, 256, 0, c.stream>>>(B.d_args, B.rec, wtot, model ? pred : nullptr, pp.cost);
-    FGSS_LAUNCH_CK();
-    exclusive_scan<uint64_t>(c, pp.cost, pp.cpre, R, nullptr, pp.cpre + R, (p + "b.scan.c").c_str());
-    k_join_cost_totals<<<grid_for(nj, 128), 128, 0, c.stream>>>(B.rec.roff, (uint32_t)nj, pp.cpre, pp.d_sums);
-    FGSS_LAUNCH_CK();
-    return pp;
+    return d_fargs;
 }
 
 // The batch's launch shape: the tuned shape of its most expensive join (the
@@ -461,6 +477,11 @@ void batched_filter_verify(Ctx& c, Batch& B, bool use_model, BatchPlan* plan) {
         }
     }
     if (nitems >= 0xffffffffull) fail(FGSS_ERR_UNSUPPORTED, "too many work items");
+    // chunk boundaries: exactly the words the splits take (the plan's size in
+    // a capture; a replay on other data that needs more bisects instead)
+    const uint64_t cbuf_cap = capture ? plan->cbuf_cap : std::min<uint64_t>(hsum[3 * nj], 0xfffffff0ull);
+    if (plan && !capture) plan->cbuf_cap = cbuf_cap;
+    FusedArgs* d_fargs = batch_filters(c, B, pp, cap_entries, cbuf_cap);
     uint32_t* hk = c.pinnedT<uint32_t>(p + "b.hkoff", nj + 1);
     hk[0] = 0;
     for (size_t i = 0; i < nj; i++) hk[i + 1] = hk[i] + K[i];
@@ -526,7 +547,7 @@ void batched_filter_verify(Ctx& c, Batch& B, bool use_model, BatchPlan* plan) {
         upload_args(c, B, p + "b.ha2");
         FGSS_CK(cudaMemsetAsync(counter, 0, (4 + nj) * 4, c.stream));
         FGSS_CK(cudaEventRecordWithFlags(c.ev[4], c.stream, rec_flags));
-        if (nitems) fused_launch(c, te, B.d_args, pp.d_fargs, items, (uint32_t)nitems, counter, sided);
+        if (nitems) fused_launch(c, te, B.d_args, d_fargs, items, (uint32_t)nitems, counter, sided);
         FGSS_CK(cudaEventRecordWithFlags(c.ev[5], c.stream, rec_flags));
         c.probe_timed = true;
         // queries deferred to the global-memory accumulator: one persistent

@@ -84,7 +84,7 @@ static __global__ void k_join_entries(const uint64_t* __restrict__ roff, uint32_
         d_e_all[2 * j] = (uint64_t)(ioff[roff[j + 1]] - ioff[roff[j]]);
 }
 
-// Warp per record: the windows of every probe token (k_windows) of every join.
+// Warp per record: the windows of every probe token (windows_query) of every join.
 static __global__ void k_windows_mj(const JoinArgs* __restrict__ joins, TileMap m, const uint32_t* __restrict__ poff,
                                     uint2* __restrict__ win, uint32_t* __restrict__ wpre, uint32_t* __restrict__ wtot,
                                     uint4* __restrict__ meta) {
@@ -110,7 +110,7 @@ static __global__ void k_bitmaps_mj(const JoinArgs* __restrict__ joins, const Fu
     }
 }
 
-// Warp per record: every join's chunk splits (k_chunks), one boundary buffer.
+// Warp per record: every join's chunk splits (chunks_query), one boundary buffer.
 static __global__ void k_chunks_mj(const JoinArgs* __restrict__ joins, const FusedArgs* __restrict__ fargs, TileMap m,
                                    const uint32_t* __restrict__ wtot, uint32_t cap, uint32_t* __restrict__ cbuf,
                                    uint64_t cbuf_cap, unsigned long long* __restrict__ cbuf_used) {
@@ -174,22 +174,30 @@ static __global__ void k_features_mj(const JoinArgs* __restrict__ joins, TileMap
 
 // Work-item cost of every query: exact window entries + 4 x the learned
 // estimate of its candidates (when given) + its size; 0 outside the join's
-// query range.
+// query range.  Also sums into *need the chunk-boundary words the queries'
+// splits for slot tables of `cap` entries take (chunks_query).
 static __global__ void k_cost_mj(const JoinArgs* __restrict__ joins, TileMap m, const uint32_t* __restrict__ wtot,
-                                 const uint32_t* __restrict__ pred, uint64_t* __restrict__ cost) {
+                                 const uint32_t* __restrict__ pred, uint32_t cap, uint64_t* __restrict__ cost,
+                                 unsigned long long* __restrict__ need) {
+    unsigned long long words = 0;
     for (uint32_t b = blockIdx.x; b < m.ntiles; b += gridDim.x) {
         const TileRange tr = tile_range(m, b);
         const JoinArgs& a = joins[tr.j];
         const uint64_t g0 = __ldg(m.roff + tr.j);
         for (uint32_t q = tr.r0 + threadIdx.x; q < tr.r1; q += blockDim.x) {
             unsigned long long v = 0;
+            const uint32_t L = wtot[g0 + q];
             if (q >= a.q_lo && q < a.q_hi) {
-                v = (unsigned long long)wtot[g0 + q] + a.len[q];
+                v = (unsigned long long)L + a.len[q];
                 if (pred) v += 4ull * pred[g0 + q];
             }
             cost[g0 + q] = v;
+            uint32_t qp, span;
+            words += (unsigned long long)(chunk_count(a, q, L, cap, qp, span) - 1) * qp;
         }
     }
+    words = warp_sum(words);
+    if (lane_id() == 0 && words) atomicAdd(need, words);
 }
 
 // Cost total of every join from the batch's exclusive cost prefix.

@@ -3,12 +3,13 @@
 // Same semantics as the plain stages (join_kernels.cuh; reference
 // filtering.cu:76-141, checking.cu:93-175, block.cu:184-197), organised for
 // throughput:
-//   * k_windows: one warp per query computes the id window [q+1, send) of
-//     every probe token's list by binary search, for all queries at once, the
-//     prefix of the window sizes and the per-query total that sizes work items.
-//   * k_chunks: queries whose windows hold more entries than half the slot
-//     table get precomputed id-range chunk boundaries.
-//   * k_bitmaps: a token bitmap per record (the bitmap filter).
+//   * windows_query: one warp per query computes the id window [q+1, send)
+//     of every probe token's list by binary search, the prefix of the window
+//     sizes and the per-query total that sizes work items (launched for every
+//     join of a batch at once by k_windows_mj, batch_kernels.cuh).
+//   * chunks_query: queries whose windows hold more entries than half the
+//     slot table get precomputed id-range chunk boundaries (k_chunks_mj).
+//   * bitmap_record: a token bitmap per record (the bitmap filter, k_bitmaps_mj).
 //   * k_fused: persistent CTAs pull work items (runs of queries of one join,
 //     longest first, claimed one item ahead).  Per query: the query's tokens
 //     and a membership structure (bitmap, hashed set or hashed bitmap) go to
@@ -35,8 +36,9 @@ struct FusedLayout {
     static constexpr uint32_t H = 1u << HLOG;
     static constexpr uint32_t cap = H / 2;    // window entries per chunk
     // probe tokens handled in shared memory: 256..512 (a slot's 11-bit query
-    // position and 10-bit match count rely on PC <= 512)
-    static constexpr uint32_t PC = H / 4 > 384 ? 384 : (H / 4 > 256 ? H / 4 : 256);
+    // position and 10-bit match count rely on PC <= 512); a query with more
+    // goes to the global-memory accumulator
+    static constexpr uint32_t PC = H / 4 > 512 ? 512 : (H / 4 > 256 ? H / 4 : 256);
     static constexpr uint32_t QC = H / 2 > 512 ? 512 : H / 2;  // query tokens staged in shared memory
                                                                   // (longer: read from HBM)
     static constexpr uint32_t BW = 1024;      // bitmap words: 32768 bits
@@ -93,6 +95,21 @@ __device__ __forceinline__ void windows_query(const JoinArgs& a, uint32_t q, con
     }
 }
 
+// Chunks of one query's id window [q+1, send) whose windows hold L entries:
+// 1 when they fit `cap`, else enough equal id ranges for 3/4 of cap on
+// average (at most one per id).  Also gives the probe prefix and the span.
+__device__ __forceinline__ uint32_t chunk_count(const JoinArgs& a, uint32_t q, uint32_t L, uint32_t cap, uint32_t& qp,
+                                                uint32_t& span) {
+    const bool unsorted = (*a.status & ST_UNSORTED) != 0;
+    const uint32_t lq = a.len[q];
+    qp = lq <= 65535u ? a.probe[lq] : 0;
+    const uint32_t send = unsorted ? a.n : (lq <= 65535u ? a.send[lq] : 0);
+    span = send > q + 1 ? send - q - 1 : 0;
+    if (L <= cap || qp == 0 || send <= q + 2) return 1;
+    const uint64_t want = ((uint64_t)L * 4 + 3ull * cap - 1) / (3ull * cap);
+    return (uint32_t)(want < span ? want : span);
+}
+
 // Chunk boundaries of one query whose windows hold more than `cap` entries
 // (warp-collective): the id window [q+1, send) is cut into nch equal id ranges
 // (sized for 3/4 of cap on average) and, for every inner boundary id b and
@@ -104,17 +121,10 @@ __device__ __forceinline__ void chunks_query(const JoinArgs& a, uint32_t q, cons
                                              uint32_t cap, uint2* __restrict__ qchunk, uint32_t* __restrict__ cbuf,
                                              uint64_t cbuf_cap, unsigned long long* __restrict__ cbuf_used) {
     const uint32_t lane = lane_id();
-    const bool unsorted = (*a.status & ST_UNSORTED) != 0;
-    const uint32_t L = wtot[q];
-    uint32_t nch = 1;
+    uint32_t qp, span;
+    uint32_t nch = chunk_count(a, q, wtot[q], cap, qp, span);
     unsigned long long base = 0;
-    const uint32_t lq = a.len[q];
-    const uint32_t qp = lq <= 65535u ? a.probe[lq] : 0;
-    const uint32_t send = unsorted ? a.n : (lq <= 65535u ? a.send[lq] : 0);
-    if (L > cap && qp > 0 && send > q + 2) {
-        const uint32_t span = send - q - 1;
-        const uint64_t want = ((uint64_t)L * 4 + 3ull * cap - 1) / (3ull * cap);
-        nch = (uint32_t)(want < span ? want : span);
+    if (nch > 1) {
         if (lane == 0) {
             const unsigned long long need = (unsigned long long)(nch - 1) * qp;
             base = atomicAdd(cbuf_used, need);

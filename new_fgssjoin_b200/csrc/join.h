@@ -147,6 +147,7 @@ struct BatchPlan {
     std::vector<uint32_t> K;          // work items per join
     uint64_t nitems = 0;
     std::vector<uint64_t> res_cap;    // result slots per join
+    uint64_t cbuf_cap = 0;            // chunk-boundary words
     uint32_t heavy_slots = 0;
 };
 // Setup of every join (join_setup_host, with the slot each JoinState holds),
