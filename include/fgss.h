@@ -194,6 +194,8 @@ typedef struct fgss_stats {
     uint64_t predicted_candidates; /* batched method with use_model: the learned model's estimates */
     uint64_t predicted_results;    /* of candidates and results (0 otherwise; compare with the exact counts) */
     uint64_t query_tokens;    /* batched method: tokens of the query records the fused kernel staged */
+    float ms_heavy;           /* batched method: the global-memory accumulator's launch alone */
+    float ms_reserved;
 } fgss_stats;
 
 typedef struct fgss_pairs {

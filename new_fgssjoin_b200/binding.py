@@ -67,7 +67,7 @@ class _Stats(ctypes.Structure):
                 ("ms_verify", ctypes.c_float), ("ms_output", ctypes.c_float), ("ms_probe", ctypes.c_float),
                 ("merged_tokens", ctypes.c_uint64), ("launches", ctypes.c_uint64),
                 ("predicted_candidates", ctypes.c_uint64), ("predicted_results", ctypes.c_uint64),
-                ("query_tokens", ctypes.c_uint64)]
+                ("query_tokens", ctypes.c_uint64), ("ms_heavy", ctypes.c_float), ("ms_reserved", ctypes.c_float)]
 
 
 class _Pairs(ctypes.Structure):

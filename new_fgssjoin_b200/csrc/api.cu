@@ -155,10 +155,10 @@ void export_batch(Ctx& c, Batch& B, const fgss_join_opts* opts, fgss_pairs* outs
 
 // Device times of a call: index build, filter+verify, output, fused launch.
 struct Times {
-    float idx = 0, fv = 0, out = 0, probe = 0;
+    float idx = 0, fv = 0, out = 0, probe = 0, heavy = 0;
 };
 
-// Adds the times the events ev[0..2] (and ev[4..5]) bracket, up to now.
+// Adds the times the events ev[0..2] (and ev[4..5], ev[6..7]) bracket, up to now.
 void add_times(Ctx& c, Times& t) {
     cudaEvent_t* ev = c.ev;
     FGSS_CK(cudaEventRecord(ev[3], c.stream));
@@ -168,6 +168,11 @@ void add_times(Ctx& c, Times& t) {
     FGSS_CK(cudaEventElapsedTime(&b, ev[1], ev[2]));
     FGSS_CK(cudaEventElapsedTime(&d, ev[2], ev[3]));
     if (c.probe_timed) FGSS_CK(cudaEventElapsedTime(&e, ev[4], ev[5]));
+    float hv = 0;
+    if (c.heavy_timed) FGSS_CK(cudaEventElapsedTime(&hv, ev[6], ev[7]));
+    c.probe_timed = false;
+    c.heavy_timed = false;
+    t.heavy += hv;
     t.idx += a;
     t.fv += b;
     t.out += d;
@@ -194,6 +199,7 @@ void report_stats(Ctx& c, std::vector<JoinState*>& js, fgss_stats* stats, unsign
             stats[i].ms_output = t.out;
             stats[i].ms_total = t.idx + t.fv + t.out;
             stats[i].ms_probe = t.probe;
+            stats[i].ms_heavy = t.heavy;
             stats[i].launches = launches;
         }
     }
@@ -298,6 +304,7 @@ bool replay_graph(Ctx& c, GraphEntry& g, const fgss_sets_view* sets, const fgss_
                   fgss_pairs* outs, fgss_stats* stats) {
     c.bpfx = g.ns;
     c.probe_timed = false;
+    c.heavy_timed = false;
     std::vector<JoinState*> v;
     for (auto& j : g.joins) v.push_back(j.get());
     Batch& B = *g.batch;
@@ -313,6 +320,7 @@ bool replay_graph(Ctx& c, GraphEntry& g, const fgss_sets_view* sets, const fgss_
     FGSS_CK(cudaGraphLaunch(g.exec, c.stream));
     launch_counter() += g.launches;
     c.probe_timed = true;
+    c.heavy_timed = g.plan.heavy_slots > 0;
     FGSS_CK(cudaEventRecord(c.ev[2], c.stream));
     uint32_t* h = c.pinnedT<uint32_t>(g.ns + "h.st", 8 * (size_t)n);
     FGSS_CK(cudaMemcpyAsync(h, B.status, 32 * (size_t)n, cudaMemcpyDeviceToHost, c.stream));
@@ -385,6 +393,7 @@ void run_joins(Ctx& c, const fgss_sets_view* sets, const fgss_join_opts* opts, i
     cudaEvent_t* ev = c.ev;
     const unsigned long long launches0 = launch_counter();
     c.probe_timed = false;
+    c.heavy_timed = false;
     Times times;
     BatchPlan plan;
     std::unique_ptr<Batch> Bp(new Batch());
@@ -724,6 +733,7 @@ fgss_status fgss_rsjoin(fgss_ctx* ctx, const fgss_sets_view* r, const fgss_sets_
         cudaEvent_t* ev = c.ev;
         const unsigned long long launches0 = launch_counter();
         c.probe_timed = false;
+        c.heavy_timed = false;
         FGSS_CK(cudaEventRecord(ev[0], c.stream));
         const RsInput u = rs_union(c, *r, *s);
         JoinState J;

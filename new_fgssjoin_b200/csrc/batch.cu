@@ -564,10 +564,13 @@ void batched_filter_verify(Ctx& c, Batch& B, bool use_model, BatchPlan* plan) {
         slots = capture ? plan->heavy_slots : plan ? all_slots : std::min<uint32_t>(max_nh, (uint32_t)c.num_sms);
         if (slots) {
             const HeavyScratch hs = heavy_scratch(c, p, B.n_max, slots, capture);
+            FGSS_CK(cudaEventRecordWithFlags(c.ev[6], c.stream, rec_flags));
             k_probe_heavy<MODE_FUSED, 512><<<slots, 512, 0, c.stream>>>(B.d_args, 0, (uint32_t)nj, hs.zero,
                                                                         hs.zero_words, hs.aux, hs.aux_words,
                                                                         counter + 4);
             FGSS_LAUNCH_CK();
+            FGSS_CK(cudaEventRecordWithFlags(c.ev[7], c.stream, rec_flags));
+            c.heavy_timed = true;
         }
         if (capture) break;
         FGSS_CK(cudaMemcpyAsync(hst, B.status, nj * 32, cudaMemcpyDeviceToHost, c.stream));

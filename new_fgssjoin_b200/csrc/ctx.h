@@ -52,6 +52,7 @@ struct Ctx {
     fgss_model* model = nullptr;
     cudaEvent_t ev[8] = {};
     bool probe_timed = false;  // ev[4]..ev[5] bracket the last fused filter+verify launch
+    bool heavy_timed = false;  // ev[6]..ev[7] bracket the last global-accumulator launch
 
     // Device buffer `name` of at least `bytes`; grows (never shrinks) and keeps
     // its address while big enough, so repeated calls at one size allocate nothing.

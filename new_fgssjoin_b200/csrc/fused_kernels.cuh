@@ -476,7 +476,9 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                             const uint32_t pos = (jv[u] << 11) | min(pv[u] & 0xffffu, kSmaxUnknown);
                             uint32_t h = hash_slot(s, hl);
                             bool done = false;
-                            unsigned long long old = kEmptySlot;  // the first try assumes an empty slot
+                            // read the slot first: 1.4 CAS per entry when the first try assumed an empty
+                            // slot (every repeat of a source failed once); a read and ~1 CAS this way
+                            unsigned long long old = *(volatile unsigned long long*)&slots[h];
                             for (uint32_t it = 0; it <= mask && !done;) {
                                 const uint32_t key = (uint32_t)(old >> 32);
                                 unsigned long long nw;
