@@ -423,7 +423,7 @@ void batch_index(Ctx& c, Batch& B, uint64_t E_cap) {
 void batch_query_costs(Ctx& c, Batch& B, bool use_model, uint64_t* out) {
     if (B.R == 0) return;
     const TuneEntry te = batch_shape(c, B);
-    const Prepass pp = batch_prepass(c, B, (1u << te.hash_log2) / 2, B.P, use_model && c.model);
+    const Prepass pp = batch_prepass(c, B, (1u << te.hash_log2) / 4 * 3, B.P, use_model && c.model);
     FGSS_CK(cudaMemcpyAsync(out, pp.cost, B.R * 8, cudaMemcpyDeviceToHost, c.stream));
     c.sync();
 }
@@ -441,7 +441,7 @@ void batched_filter_verify(Ctx& c, Batch& B, bool use_model, BatchPlan* plan) {
     const bool capture = plan && plan->capture;
     const std::string& p = c.bpfx;
     const TuneEntry te = capture ? plan->te : batch_shape(c, B);
-    const uint32_t cap_entries = (1u << te.hash_log2) / 2;  // chunk capacity of the chosen kernel shape
+    const uint32_t cap_entries = (1u << te.hash_log2) / 4 * 3;  // chunk capacity of the chosen kernel shape
     const uint64_t P_cap = plan ? plan->P_cap : B.P;
     if (P_cap < B.P) fail(FGSS_ERR_CUDA, "window buffers below the batch's probe-token count");
     const bool model = use_model && c.model;

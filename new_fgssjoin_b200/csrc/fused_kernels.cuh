@@ -7,7 +7,7 @@
 //     of every probe token's list by binary search, the prefix of the window
 //     sizes and the per-query total that sizes work items (launched for every
 //     join of a batch at once by k_windows_mj, batch_kernels.cuh).
-//   * chunks_query: queries whose windows hold more entries than half the
+//   * chunks_query: queries whose windows hold more entries than 3/4 of the
 //     slot table get precomputed id-range chunk boundaries (k_chunks_mj).
 //   * bitmap_record: a token bitmap per record (the bitmap filter, k_bitmaps_mj).
 //   * k_fused: persistent CTAs pull work items (runs of queries of one join,
@@ -34,7 +34,7 @@ constexpr uint32_t kSmaxUnknown = 2047;
 template <int HLOG>
 struct FusedLayout {
     static constexpr uint32_t H = 1u << HLOG;
-    static constexpr uint32_t cap = H / 2;    // window entries per chunk
+    static constexpr uint32_t cap = H / 4 * 3;  // window entries per chunk (load <= 3/4)
     // probe tokens handled in shared memory: 256..512 (a slot's 11-bit query
     // position and 10-bit match count rely on PC <= 512); a query with more
     // goes to the global-memory accumulator

@@ -147,3 +147,22 @@ def batch_sizes(n_joins=256, lo=1000, hi=200000, seed=0):
 # tokenization of the workloads: padded lower-case 3-grams, distinct per record
 TITLE_TOK = dict(q=3, mode="qgram", pad=True, suffix=False, lower=True)
 READ_TOK = dict(q=16, mode="kmer", pad=False, suffix=False, lower=True)
+
+
+def main(argv=None):
+    """Writes one of the synthetic workloads' texts to a file (one record per line):
+    python -m new_fgssjoin_b200.datagen heavy|titles <records> [--seed S] --out <path>."""
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m new_fgssjoin_b200.datagen")
+    ap.add_argument("kind", choices=["heavy", "titles"])
+    ap.add_argument("records", type=int)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--out", required=True)
+    a = ap.parse_args(argv)
+    text = (heavy if a.kind == "heavy" else titles)(a.records, seed=a.seed)
+    with open(a.out, "wb") as f:
+        f.write(text if isinstance(text, (bytes, bytearray)) else text.encode())
+
+
+if __name__ == "__main__":
+    main()
