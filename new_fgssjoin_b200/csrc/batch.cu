@@ -54,6 +54,7 @@ int fused_resident_ctas(Ctx& c, const TuneEntry& te) {
     FGSS_R(128, 10, 1024)
     FGSS_R(128, 10, 768)
     FGSS_R(128, 11, 768)
+    FGSS_R(128, 11, 896)
     FGSS_R(256, 11, 768)
     FGSS_R(256, 12, 768)
 #undef FGSS_R
@@ -83,8 +84,8 @@ static void launch_fused(Ctx& c, const JoinArgs* d_args, const FusedArgs* d_farg
 // resident threads per SM the register budget is sized for.
 extern const int kFusedShapes[][3] = {{32, 8, 1024},  {32, 9, 1024},  {64, 9, 1024},   {64, 9, 768},
                                       {64, 10, 1024}, {128, 9, 1024}, {128, 10, 1024}, {128, 10, 768},
-                                      {128, 11, 768}, {256, 11, 768},  {256, 12, 768}};
-extern const int kNumFusedShapes = 11;
+                                      {128, 11, 768}, {256, 11, 768},  {256, 12, 768}, {128, 11, 896}};
+extern const int kNumFusedShapes = 12;
 
 // The launch shape that stands for a requested filter strategy.
 TuneEntry filter_entry(int filter) {
@@ -120,6 +121,7 @@ void fused_launch(Ctx& c, const TuneEntry& te, const JoinArgs* d_args, const Fus
     FGSS_F(128, 10, 1024)
     FGSS_F(128, 10, 768)
     FGSS_F(128, 11, 768)
+    FGSS_F(128, 11, 896)
     FGSS_F(256, 11, 768)
     FGSS_F(256, 12, 768)
 #undef FGSS_F

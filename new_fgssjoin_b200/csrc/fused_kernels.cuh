@@ -29,19 +29,24 @@ namespace fgss {
 // number of prefix matches (10).
 constexpr uint32_t kSmaxUnknown = 2047;
 
+// The query's membership structure (bitmap, hashed set or hashed bitmap): 2^kMemberBits bits.
+constexpr uint32_t kMemberBits = 14;
+constexpr uint32_t kMemberWords = 1u << (kMemberBits - 5);
+
 // Layout: slots u64[H] | occ u16[H] | sls u16[H] | clo u32[PC] |
 //         wpre u32[PC+4] | qtok u32[QC] | bm u32[BW] | mlist u16[MC]
 template <int HLOG>
 struct FusedLayout {
     static constexpr uint32_t H = 1u << HLOG;
     static constexpr uint32_t cap = H / 4 * 3;  // window entries per chunk (load <= 3/4)
-    // probe tokens handled in shared memory: 256..512 (a slot's 11-bit query
+    // probe tokens handled in shared memory: 256..384 (a slot's 11-bit query
     // position and 10-bit match count rely on PC <= 512); a query with more
-    // goes to the global-memory accumulator
-    static constexpr uint32_t PC = H / 4 > 512 ? 512 : (H / 4 > 256 ? H / 4 : 256);
-    static constexpr uint32_t QC = H / 2 > 512 ? 512 : H / 2;  // query tokens staged in shared memory
+    // goes to the global-memory accumulator.  The staging caps keep the
+    // 2^11-slot table at 31 KB, 7 CTAs of 128 threads per SM
+    static constexpr uint32_t PC = H / 4 > 384 ? 384 : (H / 4 > 256 ? H / 4 : 256);
+    static constexpr uint32_t QC = H / 2 > 256 ? 256 : H / 2;  // query tokens staged in shared memory
                                                                   // (longer: read from HBM)
-    static constexpr uint32_t BW = 1024;      // bitmap words: 32768 bits
+    static constexpr uint32_t BW = kMemberWords;  // membership words: 16384 bits
     static constexpr uint32_t MC = 256;       // merge list entries per chunk (more: merged by their lane)
     static constexpr size_t off_occ = 8ull * H;
     static constexpr size_t off_sls = off_occ + 2ull * H;   // source size of each slot
@@ -160,14 +165,16 @@ struct FusedArgs {
 
 // Query-token membership, three forms chosen per query (the same for every
 // thread of the CTA):
-//   QM_EXACT  vocabulary of at most 32768 terms: one bit per term;
-//   QM_HASH   larger vocabulary, query of at most 512 tokens: open-addressing
-//             set of token + 1 in the same 1024 words (load <= 1/2, 0 = empty);
+//   QM_EXACT  vocabulary of at most 2^kMemberBits terms: one bit per term;
+//   QM_HASH   larger vocabulary, query of at most kQHashMax tokens: open-addressing
+//             set of token + 1 in the same kMemberWords words (load <= 1/2, 0 = empty);
 //   QM_BLOOM  otherwise: one bit per hash, hits confirmed by binary search.
 enum : uint32_t { QM_EXACT = 0, QM_HASH = 1, QM_BLOOM = 2 };
-constexpr uint32_t kQHashWords = 1024, kQHashMax = 512;
+constexpr uint32_t kQHashBits = kMemberBits - 5, kQHashWords = 1u << kQHashBits, kQHashMax = kQHashWords / 2;
 
-__device__ __forceinline__ uint32_t qhash(uint32_t x) { return (x * 0x9E3779B1u) >> 22; }  // 10 bits
+// Start slot of token x in the hashed set; bit of x in the hashed bitmap.
+__device__ __forceinline__ uint32_t qhash(uint32_t x) { return (x * 0x9E3779B1u) >> (32 - kQHashBits); }
+__device__ __forceinline__ uint32_t bloom_bit(uint32_t x) { return (x * 0x9E3779B1u) >> (32 - kMemberBits); }
 
 __device__ __forceinline__ bool bm_test(const uint32_t* bm, uint32_t mode, uint32_t x, const uint32_t* qtok,
                                         uint32_t qa, uint32_t lq) {
@@ -181,7 +188,7 @@ __device__ __forceinline__ bool bm_test(const uint32_t* bm, uint32_t mode, uint3
         }
         return false;
     }
-    const uint32_t b = mode == QM_EXACT ? x : ((x * 0x9E3779B1u) >> 17);
+    const uint32_t b = mode == QM_EXACT ? x : bloom_bit(x);
     bool hit = (bm[b >> 5] >> (b & 31)) & 1u;
     if (hit && mode != QM_EXACT) hit = contains_gen(qtok, qa, lq, x);
     return hit;
@@ -198,7 +205,7 @@ __device__ __forceinline__ void bm_insert(uint32_t* bm, uint32_t mode, uint32_t 
         }
         return;
     }
-    const uint32_t b = mode == QM_EXACT ? x : ((x * 0x9E3779B1u) >> 17);
+    const uint32_t b = mode == QM_EXACT ? x : bloom_bit(x);
     atomicOr(&bm[b >> 5], 1u << (b & 31));
 }
 
@@ -645,7 +652,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     } else {
         for (uint32_t j = tid; j < lq; j += NT) {
             const uint32_t x = qsrc[j];
-            const uint32_t b = qmode == QM_EXACT ? x : ((x * 0x9E3779B1u) >> 17);
+            const uint32_t b = qmode == QM_EXACT ? x : bloom_bit(x);
             bm[b >> 5] = 0u;
         }
     }
