@@ -220,8 +220,12 @@ fgss_status fgss_selfjoin(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_
                           fgss_pairs* out, fgss_stats* stats);
 
 /* Many independent self-joins (each with its own sets and threshold) in one
- * persistent launch per stage.  outs and stats are arrays of n (stats may be
- * NULL).  No reference counterpart: it runs process_blocks once per join. */
+ * launch per stage for the whole batch with the batched method (prefix
+ * lengths, index, pre-pass, work items, the persistent fused filter+verify
+ * kernel, result sort and output; a batch whose tokens or records exceed the
+ * 32-bit batch offsets runs as consecutive groups).  outs and stats are arrays
+ * of n (stats may be NULL).  No reference counterpart: it runs process_blocks
+ * once per join. */
 fgss_status fgss_selfjoin_batch(fgss_ctx* ctx, const fgss_sets_view* sets, const fgss_join_opts* opts,
                                 int n, fgss_pairs* outs, fgss_stats* stats);
 

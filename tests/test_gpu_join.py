@@ -169,6 +169,51 @@ def test_batch_of_joins_equals_single_joins(ctx):
         _check_same(got, ref, st)
 
 
+def _long_and_short_records(seed):
+    """A few records longer than the fused kernel's probe cap among short ones."""
+    rng = np.random.default_rng(seed)
+    base = rng.choice(8000, size=3000, replace=False)
+    recs = [np.sort(np.delete(base, rng.choice(3000, size=int(rng.integers(0, 300)), replace=False)))
+            for _ in range(12)]
+    recs += [np.sort(rng.choice(8000, size=int(rng.integers(5, 60)), replace=False)) for _ in range(150)]
+    return _sets_of(recs, 8000)
+
+
+def test_batch_stage_launches_cover_every_join_kind(ctx):
+    """One batched call whose per-stage launches span joins of every kind at once: empty,
+    a single record, records without any pair, long records for the global accumulator,
+    and title joins of several sizes and thresholds; every join equals its own oracle join
+    and the launches do not grow with the number of joins."""
+    empty = F.Sets(np.zeros(0), np.zeros(0), np.zeros(0), np.zeros(0), 0)
+    one = F.Sets([7], [0], [3], [1, 2, 3], 4)
+    disjoint = F.Sets([1, 2, 3], [0, 3, 6], [3, 3, 3], [0, 1, 2, 3, 4, 5, 6, 7, 8], 9)
+    titles = [ctx.tokenize(_titles(n, 300 + n), **datagen.TITLE_TOK) for n in (700, 2200, 1300)]
+    sets = [titles[0], empty, _long_and_short_records(8), one, titles[1], disjoint, titles[2]]
+    ts = [0.6, 0.7, 0.7, 0.5, 0.9, 0.5, 0.8]
+    outs = ctx.selfjoin_batch(sets, ts, method="batched")
+    for s, t, got in zip(sets, ts, outs):
+        ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, t)
+        _check_same(got, ref, st)
+    assert outs[2].stats["heavy_queries"] > 0
+    few = ctx.selfjoin_batch(sets[:2], ts[:2], method="batched")[0].stats["launches"]
+    # the same stages whatever the number of joins: only sort passes (wider keys) and the
+    # global accumulator's launch come on top, where per-join stages would add about 75
+    assert outs[0].stats["launches"] <= few + 30
+
+
+def test_batch_of_many_small_joins(ctx):
+    """Sixty joins in one call: the tile maps over many joins, with a shared host input."""
+    base = ctx.tokenize(_titles(400, 77), **datagen.TITLE_TOK)
+    small = [ctx.tokenize(_titles(int(n), 500 + i), **datagen.TITLE_TOK)
+             for i, n in enumerate(np.linspace(20, 600, 30))]
+    sets = [x for pair in zip(small, [base] * 30) for x in pair]
+    ts = [0.5 + 0.45 * (i % 7) / 6 for i in range(len(sets))]
+    outs = ctx.selfjoin_batch(sets, ts, method="batched")
+    for s, t, got in zip(sets, ts, outs):
+        ref, st = O.join(s.pos, s.len, s.tokens, s.n_terms, t)
+        _check_same(got, ref, st)
+
+
 def test_batch_sharing_host_arrays(ctx, titles_sets):
     """Joins of one batched call on the same host arrays (copied to the device once)."""
     s = titles_sets
