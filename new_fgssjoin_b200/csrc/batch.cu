@@ -176,7 +176,7 @@ unsigned tile_grid(Ctx& c, const TileMap& m, unsigned per_sm = 16) {
 
 template <typename K>
 void index_sort(Ctx& c, Batch& B, uint64_t E_cap, int tbits, int jbits, const uint64_t* d_E, const uint64_t* d_loff,
-                uint32_t* list, uint32_t* ent_s, uint32_t* ent_pl) {
+                uint32_t* list, uint2* ent) {
     const std::string& p = c.bpfx;
     K* key = c.devT<K>(p + "b.ix.key", E_cap + 1);
     uint64_t* val = c.devT<uint64_t>(p + "b.ix.val", E_cap + 1);
@@ -185,7 +185,7 @@ void index_sort(Ctx& c, Batch& B, uint64_t E_cap, int tbits, int jbits, const ui
     FGSS_LAUNCH_CK();
     radix_sort<K, uint64_t>(c, key, val, E_cap, d_E, 0, tbits + jbits, (p + "b.ixsort").c_str());
     k_index_lists_mj<K><<<grid_for(E_cap, 256, c.num_sms * 32), 256, 0, c.stream>>>(
-        B.d_args, key, val, d_E, (uint32_t)tbits, d_loff, list, ent_s, ent_pl);
+        B.d_args, key, val, d_E, (uint32_t)tbits, d_loff, list, ent);
     FGSS_LAUNCH_CK();
 }
 
@@ -399,13 +399,11 @@ void batch_index(Ctx& c, Batch& B, uint64_t E_cap) {
     uint64_t* d_loff = c.devT<uint64_t>(p + "b.loff", nj + 1);
     FGSS_CK(cudaMemcpyAsync(d_loff, hl, (nj + 1) * 8, cudaMemcpyHostToDevice, c.stream));
     uint32_t* list = c.devT<uint32_t>(p + "b.list", L + 1);
-    uint32_t* ent_s = c.devT<uint32_t>(p + "b.ent_s", E_cap + 1);
-    uint32_t* ent_pl = c.devT<uint32_t>(p + "b.ent_pl", E_cap + 1);
+    uint2* ent = c.devT<uint2>(p + "b.ent", E_cap + 1);
     for (size_t j = 0; j < nj; j++) {
         JoinArgs& a = B.js[j]->args;
         a.list_off = list + hl[j];
-        a.ent_s = ent_s;
-        a.ent_pl = ent_pl;
+        a.ent = ent;
     }
     // a join without entries keeps these zero offsets (empty lists)
     FGSS_CK(cudaMemsetAsync(list, 0, L * 4, c.stream));
@@ -416,8 +414,8 @@ void batch_index(Ctx& c, Batch& B, uint64_t E_cap) {
         FGSS_LAUNCH_CK();
         k_join_entries<<<grid_for(nj, 128), 128, 0, c.stream>>>(B.rec.roff, (uint32_t)nj, B.ioff, B.d_e);
         FGSS_LAUNCH_CK();
-        if (tbits + jbits <= 32) index_sort<uint32_t>(c, B, E_cap, tbits, jbits, d_E, d_loff, list, ent_s, ent_pl);
-        else index_sort<uint64_t>(c, B, E_cap, tbits, jbits, d_E, d_loff, list, ent_s, ent_pl);
+        if (tbits + jbits <= 32) index_sort<uint32_t>(c, B, E_cap, tbits, jbits, d_E, d_loff, list, ent);
+        else index_sort<uint64_t>(c, B, E_cap, tbits, jbits, d_E, d_loff, list, ent);
     }
     upload_args(c, B, p + "b.ha1");
 }

@@ -59,14 +59,12 @@ template <typename K>
 __global__ void k_index_lists_mj(const JoinArgs* __restrict__ joins, const K* __restrict__ key,
                                         const uint64_t* __restrict__ val, const uint64_t* __restrict__ d_e,
                                         uint32_t tbits, const uint64_t* __restrict__ loff,
-                                        uint32_t* __restrict__ list_all, uint32_t* __restrict__ ent_s,
-                                        uint32_t* __restrict__ ent_pl) {
+                                        uint32_t* __restrict__ list_all, uint2* __restrict__ ent) {
     const uint64_t E = *d_e;
     const uint64_t tmask = (1ull << tbits) - 1;
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < E; k += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t v = val[k], kk = (uint64_t)key[k];
-        ent_s[k] = (uint32_t)(v >> 32);
-        ent_pl[k] = (uint32_t)v;
+        ent[k] = make_uint2((uint32_t)(v >> 32), (uint32_t)v);
         const uint32_t j = (uint32_t)(kk >> tbits), w = (uint32_t)(kk & tmask);
         uint32_t* lo = list_all + loff[j];
         if (k == 0 || (uint32_t)((uint64_t)key[k - 1] >> tbits) != j)

@@ -83,8 +83,8 @@ __device__ __forceinline__ void windows_query(const JoinArgs& a, uint32_t q, con
             lo = e;
             hi = e;
             if (send > q + 1) {
-                lo = lower_bound_u32(a.ent_s, b, e, q + 1);
-                hi = unsorted ? e : lower_bound_u32(a.ent_s, lo, e, send);
+                lo = lower_bound_src(a.ent, b, e, q + 1);
+                hi = unsorted ? e : lower_bound_src(a.ent, lo, e, send);
             }
         }
         const uint32_t incl = warp_incl_scan(hi - lo);
@@ -144,7 +144,7 @@ __device__ __forceinline__ void chunks_query(const JoinArgs& a, uint32_t q, cons
                 const uint32_t i = f / qp + 1, j = f % qp;
                 const uint32_t b = q + 1 + (uint32_t)(((uint64_t)span * i) / nch);
                 const uint2 wj = w[j];
-                cbuf[base + f] = lower_bound_u32(a.ent_s, wj.x, wj.y, b);
+                cbuf[base + f] = lower_bound_src(a.ent, wj.x, wj.y, b);
             }
         }
     }
@@ -406,8 +406,8 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                                     hi = tag + 1 == nch ? qwin[j].y : cb[tag * qp + j];
                                 } else {
                                     const uint2 wj = qwin[j];
-                                    lo = lower_bound_u32(a.ent_s, wj.x, wj.y, ra);
-                                    hi = lower_bound_u32(a.ent_s, lo, wj.y, rb);
+                                    lo = lower_bound_src(a.ent, wj.x, wj.y, ra);
+                                    hi = lower_bound_src(a.ent, lo, wj.y, rb);
                                 }
                                 cnt = hi - lo;
                                 clo[j] = lo;
@@ -465,8 +465,9 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                             j = lo2 - 1;
                         }
                         const uint32_t k = clo[j] + (f - wpre[j]);
-                        sv[u] = __ldg(a.ent_s + k);
-                        pv[u] = __ldg(a.ent_pl + k);  // source size << 16 | source position
+                        const uint2 e = __ldg(a.ent + k);  // one 8-byte entry
+                        sv[u] = e.x;
+                        pv[u] = e.y;  // source size << 16 | source position
                         jv[u] = j;
                     }
                 }

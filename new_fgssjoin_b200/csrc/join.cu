@@ -194,11 +194,9 @@ void join_index(Ctx& c, JoinState& J) {
     uint32_t* ioff = c.devT<uint32_t>(J.pfx("ioff"), n + 1);
     uint32_t* e32 = c.devT<uint32_t>(J.pfx("E32"), 2);
     uint32_t* list_off = c.devT<uint32_t>(J.pfx("list_off"), (uint64_t)J.in.n_terms + 2);
-    uint32_t* ent_s = c.devT<uint32_t>(J.pfx("ent_s"), T + 1);
-    uint32_t* ent_pl = c.devT<uint32_t>(J.pfx("ent_pl"), T + 1);
+    uint2* ent = c.devT<uint2>(J.pfx("ent"), T + 1);
     a.list_off = list_off;
-    a.ent_s = ent_s;
-    a.ent_pl = ent_pl;
+    a.ent = ent;
     if (n == 0) {
         FGSS_CK(cudaMemsetAsync(list_off, 0, ((uint64_t)J.in.n_terms + 1) * 4, c.stream));
         FGSS_CK(cudaMemsetAsync(J.d_e, 0, 8, c.stream));
@@ -214,7 +212,7 @@ void join_index(Ctx& c, JoinState& J) {
     FGSS_LAUNCH_CK();
     radix_sort<uint32_t, uint64_t>(c, key, val, T, J.d_e, 0, J.term_bits, J.pfx("ixsort").c_str());
     k_index_lists<<<grid_for(T, 256, c.num_sms * 32), 256, 0, c.stream>>>(key, val, J.d_e, J.in.n_terms, list_off,
-                                                                         ent_s, ent_pl);
+                                                                         ent);
     FGSS_LAUNCH_CK();
 }
 

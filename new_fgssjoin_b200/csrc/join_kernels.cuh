@@ -79,8 +79,8 @@ struct JoinArgs {
     float thr;                 // the join's threshold
     // inverted index
     const uint32_t* list_off;  // [n_terms + 1]
-    const uint32_t* ent_s;     // source record of each entry, ascending within a list
-    const uint32_t* ent_pl;    // source size << 16 | position of the token in the source
+    const uint2* ent;          // per entry: (source record, source size << 16 | position of the token
+                               // in the source); sources ascending within a list
     // plain method
     uint32_t* vcnt;            // count pass: per query, candidates that need a merge
     uint32_t* ccnt;            // count pass: per query, candidates (reference definition)
@@ -114,6 +114,16 @@ __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* __restrict__
     while (lo < hi) {
         uint32_t mid = (lo + hi) >> 1;
         if (__ldg(a + mid) < x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// first entry in [lo, hi) whose source is >= x (sources ascending)
+__device__ __forceinline__ uint32_t lower_bound_src(const uint2* __restrict__ e, uint32_t lo, uint32_t hi, uint32_t x) {
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(&e[mid].x) < x) lo = mid + 1;
         else hi = mid;
     }
     return lo;
@@ -282,10 +292,10 @@ static __global__ void k_index_entries(JoinArgs a, const uint32_t* __restrict__ 
 }
 
 // After the stable sort by term: list offsets (no atomics: the thread at each
-// term boundary fills the offsets of the terms it spans) and the SoA split.
+// term boundary fills the offsets of the terms it spans) and the 8-byte entries.
 static __global__ void k_index_lists(const uint32_t* __restrict__ key, const uint64_t* __restrict__ val,
                               const uint64_t* __restrict__ d_e, uint32_t n_terms, uint32_t* __restrict__ list_off,
-                              uint32_t* __restrict__ ent_s, uint32_t* __restrict__ ent_pl) {
+                              uint2* __restrict__ ent) {
     const uint32_t E = (uint32_t)*d_e;
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -295,8 +305,7 @@ static __global__ void k_index_lists(const uint32_t* __restrict__ key, const uin
     }
     for (uint32_t k = tid; k < E; k += stride) {
         uint64_t v = val[k];
-        ent_s[k] = (uint32_t)(v >> 32);
-        ent_pl[k] = (uint32_t)v;
+        ent[k] = make_uint2((uint32_t)(v >> 32), (uint32_t)v);
         uint32_t w = key[k];
         if (k == 0)
             for (uint32_t x = 0; x <= w; x++) list_off[x] = 0;
@@ -533,8 +542,8 @@ __device__ void probe_query_smem(const JoinArgs& a, uint32_t q, unsigned char* s
     for (uint32_t j = tid; j < qp; j += NT) {
         uint32_t w = qtok[j];
         uint32_t b = __ldg(a.list_off + w), e = __ldg(a.list_off + w + 1);
-        uint32_t lo = lower_bound_u32(a.ent_s, b, e, q + 1);
-        uint32_t hi = unsorted ? e : lower_bound_u32(a.ent_s, lo, e, send);
+        uint32_t lo = lower_bound_src(a.ent, b, e, q + 1);
+        uint32_t hi = unsorted ? e : lower_bound_src(a.ent, lo, e, send);
         wlo[j] = lo;
         whi[j] = hi;
     }
@@ -564,8 +573,8 @@ __device__ void probe_query_smem(const JoinArgs& a, uint32_t q, unsigned char* s
                 uint32_t cnt = 0;
                 if (j < qp) {
                     const uint32_t lo0 = wlo[j], hi0 = whi[j];
-                    const uint32_t lo = (ra == q + 1) ? lo0 : lower_bound_u32(a.ent_s, lo0, hi0, ra);
-                    const uint32_t hi = (rb == send) ? hi0 : lower_bound_u32(a.ent_s, lo, hi0, rb);
+                    const uint32_t lo = (ra == q + 1) ? lo0 : lower_bound_src(a.ent, lo0, hi0, ra);
+                    const uint32_t hi = (rb == send) ? hi0 : lower_bound_src(a.ent, lo, hi0, rb);
                     cnt = hi - lo;
                     clo[j] = lo;
                 }
@@ -609,7 +618,7 @@ __device__ void probe_query_smem(const JoinArgs& a, uint32_t q, unsigned char* s
         for (uint32_t f = tid; f < L; f += NT) {
             const uint32_t j = upper_bound_gen(wpre, 0, qp, f) - 1;
             const uint32_t k = clo[j] + (f - wpre[j]);
-            const uint32_t s = __ldg(a.ent_s + k);
+            const uint32_t s = __ldg(&a.ent[k].x);
             if (unsorted && !size_ok(a, lq, a.len[s])) continue;
             if (a.side && __ldg(a.side + s) == __ldg(a.side + q)) continue;
             if (!slot_add(slots, mask, hl, s, j)) atomicOr(a.status, ST_HASH_FULL);
@@ -789,8 +798,8 @@ __global__ void __launch_bounds__(NT) k_probe_heavy(const JoinArgs* __restrict__
                 for (uint32_t j = tid; j < qp; j += NT) {
                     uint32_t w = __ldg(qt + j);
                     uint32_t b = __ldg(a.list_off + w), e = __ldg(a.list_off + w + 1);
-                    uint32_t lo = lower_bound_u32(a.ent_s, b, e, q + 1);
-                    uint32_t hi = unsorted ? e : lower_bound_u32(a.ent_s, lo, e, max(send, q + 1));
+                    uint32_t lo = lower_bound_src(a.ent, b, e, q + 1);
+                    uint32_t hi = unsorted ? e : lower_bound_src(a.ent, lo, e, max(send, q + 1));
                     wlo[j] = lo;
                     wpre[j] = hi - lo;
                 }
@@ -817,8 +826,9 @@ __global__ void __launch_bounds__(NT) k_probe_heavy(const JoinArgs* __restrict__
                 for (uint32_t f = tid; f < L; f += NT) {
                     uint32_t j = upper_bound_gen(wpre, 0, qp, f) - 1;
                     uint32_t k = wlo[j] + (f - wpre[j]);
-                    uint32_t s = __ldg(a.ent_s + k);
-                    uint32_t sp = __ldg(a.ent_pl + k) & 0xffffu;
+                    const uint2 e = __ldg(a.ent + k);
+                    uint32_t s = e.x;
+                    uint32_t sp = e.y & 0xffffu;
                     if (unsorted && !size_ok(a, lq, a.len[s])) continue;
                     if (a.side && __ldg(a.side + s) == __ldg(a.side + q)) continue;
                     uint32_t old = atomicAdd(&gcnt[s], 1u);
