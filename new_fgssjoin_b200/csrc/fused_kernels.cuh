@@ -33,8 +33,14 @@ constexpr uint32_t kSmaxUnknown = 2047;
 constexpr uint32_t kMemberBits = 14;
 constexpr uint32_t kMemberWords = 1u << (kMemberBits - 5);
 
-// Layout: slots u64[H] | occ u16[H] | sls u16[H] | clo u32[PC] |
-//         wpre u32[PC+4] | qtok u32[QC] | bm u32[BW] | mlist u16[MC]
+// Layout: slots u64[H] | occ u16[H] | sls u16[H] | cbr u32[PC] | jr u16[PC] |
+//         sbits u32[JW] | gpre u16[JW] | qtok u32[QC] | bm u32[BW] | mlist u16[MC]
+// The current part's windows are kept in rank form: its non-empty windows in
+// order get ranks r, cbr[r] = first entry - entries of the earlier windows
+// (so entry f of the part is ent[cbr[r] + f]) and jr[r] = the probe position;
+// bit f of sbits is set where a window starts, gpre[g] = windows starting
+// before entry 32 g.  Entry f's window is then rank gpre[f / 32] - 1 plus the
+// starts at or below f in its group: two broadcast loads and a popcount.
 template <int HLOG>
 struct FusedLayout {
     static constexpr uint32_t H = 1u << HLOG;
@@ -46,13 +52,20 @@ struct FusedLayout {
     static constexpr uint32_t PC = H / 4 > 384 ? 384 : (H / 4 > 256 ? H / 4 : 256);
     static constexpr uint32_t QC = H / 2 > 256 ? 256 : H / 2;  // query tokens staged in shared memory
                                                                   // (longer: read from HBM)
+    // entries of one part: at most cap, or PC when a part of one source id
+    // (which holds at most one entry per probe window) cannot be bisected
+    static constexpr uint32_t JE = cap > PC ? cap : PC;
+    static constexpr uint32_t JW = (JE + 31) / 32;  // groups of 32 entries
     static constexpr uint32_t BW = kMemberWords;  // membership words: 16384 bits
     static constexpr uint32_t MC = 256;       // merge list entries per chunk (more: merged by their lane)
+    static constexpr size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
     static constexpr size_t off_occ = 8ull * H;
     static constexpr size_t off_sls = off_occ + 2ull * H;   // source size of each slot
-    static constexpr size_t off_clo = off_sls + 2ull * H;
-    static constexpr size_t off_wpre = off_clo + 4ull * PC;
-    static constexpr size_t off_qtok = off_wpre + 4ull * (PC + 4);
+    static constexpr size_t off_cbr = off_sls + 2ull * H;
+    static constexpr size_t off_jr = off_cbr + 4ull * PC;
+    static constexpr size_t off_sbits = al16(off_jr + 2ull * PC);
+    static constexpr size_t off_gpre = off_sbits + 4ull * JW;
+    static constexpr size_t off_qtok = al16(off_gpre + 2ull * JW);
     static constexpr size_t off_bm = off_qtok + 4ull * QC;
     static constexpr size_t off_ml = off_bm + 4ull * BW;
     static constexpr size_t bytes = off_ml + 2ull * MC;
@@ -297,8 +310,10 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem);
     uint16_t* occ = reinterpret_cast<uint16_t*>(smem + Lay::off_occ);
     uint16_t* sls = reinterpret_cast<uint16_t*>(smem + Lay::off_sls);
-    uint32_t* clo = reinterpret_cast<uint32_t*>(smem + Lay::off_clo);
-    uint32_t* wpre = reinterpret_cast<uint32_t*>(smem + Lay::off_wpre);
+    uint32_t* cbr = reinterpret_cast<uint32_t*>(smem + Lay::off_cbr);
+    uint16_t* jr = reinterpret_cast<uint16_t*>(smem + Lay::off_jr);
+    uint32_t* sbits = reinterpret_cast<uint32_t*>(smem + Lay::off_sbits);
+    uint16_t* gpre = reinterpret_cast<uint16_t*>(smem + Lay::off_gpre);
     uint32_t* qtok = reinterpret_cast<uint32_t*>(smem + Lay::off_qtok);
     uint32_t* bm = reinterpret_cast<uint32_t*>(smem + Lay::off_bm);
     uint16_t* mlist = reinterpret_cast<uint16_t*>(smem + Lay::off_ml);
@@ -342,13 +357,47 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     // one chunk that fits the slot table (the common case): the pre-pass's
     // window prefix is used as is, with no block-wide scan
     const bool one_chunk = nch == 1 && qm.w <= Lay::cap;
-    const uint32_t* qpre = fa.wpre + fa.poff[q];
-    for (uint32_t j = tid; j < qp; j += NT) {
-        if (one_chunk) {
-            clo[j] = qwin[j].x;
-            wpre[j] = qpre[j];
+    // Warp-collective (warp 0): lays out a part's windows in rank form from
+    // bounds(j) = (first entry, end) of probe window j inside the part; returns
+    // the part's entries.  A part of more than JE entries is bisected by the
+    // caller and its layout never read (starts past JE are not marked).
+    auto lay_windows = [&](auto&& bounds) -> uint32_t {
+        for (uint32_t g = lane; g < Lay::JW; g += 32) sbits[g] = 0u;
+        __syncwarp();
+        uint32_t carry = 0, rc = 0;
+        for (uint32_t j0 = 0; j0 < qp; j0 += 32) {
+            const uint32_t j = j0 + lane;
+            uint32_t lo = 0, cnt = 0;
+            if (j < qp) {
+                const uint2 b = bounds(j);
+                lo = b.x;
+                cnt = b.y - b.x;
+            }
+            const uint32_t incl = warp_incl_scan(cnt);
+            const uint32_t p = carry + incl - cnt;  // entries of the earlier windows
+            const uint32_t nz = __ballot_sync(kFull, cnt != 0);
+            if (cnt != 0) {
+                const uint32_t r = rc + __popc(nz & lanemask_lt());
+                cbr[r] = lo - p;
+                jr[r] = (uint16_t)j;
+                if (p < Lay::JW * 32) atomicOr(&sbits[p >> 5], 1u << (p & 31));
+            }
+            carry += __shfl_sync(kFull, incl, 31);
+            rc += __popc(nz);
         }
-    }
+        __syncwarp();
+        const uint32_t ng = min((carry + 31) / 32, Lay::JW);
+        uint32_t gc = 0;
+        for (uint32_t g0 = 0; g0 < ng; g0 += 32) {
+            const uint32_t g = g0 + lane;
+            const uint32_t c = g < ng ? __popc(sbits[g]) : 0u;
+            const uint32_t incl = warp_incl_scan(c);
+            if (g < ng) gpre[g] = (uint16_t)(gc + incl - c);
+            gc += __shfl_sync(kFull, incl, 31);
+        }
+        return carry;
+    };
+    if (one_chunk && wid == 0) lay_windows([&](uint32_t j) { return qwin[j]; });
     if (tid == 0) {
         s_cand = 0;
         s_win = 0;
@@ -356,13 +405,12 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
         s_nocc = 0;
         s_nm = 0;
         ctr.qtok += lq;
-        if (one_chunk) wpre[qp] = qm.w;
     }
     const uint4* smin = fa.smin + lq;  // indexed by the source size
     // The chunks of the query's id window: a single chunk when its windows fit
     // the slot table, else the precomputed split, whose parts bisect
     // themselves further while they hold more than `cap` entries.  A chunk's
-    // windows are in clo / wpre (wpre[qp] = L entries) before it is
+    // windows are laid out in rank form (cbr, jr, sbits, gpre) before it is
     // accumulated, decided and merged.
     const uint32_t span = send - q - 1;
     const uint32_t n_parts = one_chunk ? 1u : nch;
@@ -395,27 +443,16 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                     if (sp == 0) {
                         if (lane == 0) s_L = kNoPart;
                     } else {
-                        uint32_t carry = 0;
-                        for (uint32_t j0 = 0; j0 < qp; j0 += 32) {
-                            const uint32_t j = j0 + lane;
-                            uint32_t cnt = 0;
-                            if (j < qp) {
-                                uint32_t lo, hi;
-                                if (tag != 0xffffffffu) {
-                                    lo = tag == 0 ? qwin[j].x : cb[(tag - 1) * qp + j];
-                                    hi = tag + 1 == nch ? qwin[j].y : cb[tag * qp + j];
-                                } else {
-                                    const uint2 wj = qwin[j];
-                                    lo = lower_bound_src(a.ent, wj.x, wj.y, ra);
-                                    hi = lower_bound_src(a.ent, lo, wj.y, rb);
-                                }
-                                cnt = hi - lo;
-                                clo[j] = lo;
+                        const uint32_t carry = lay_windows([&](uint32_t j) {
+                            if (tag != 0xffffffffu) {
+                                const uint32_t lo = tag == 0 ? qwin[j].x : cb[(tag - 1) * qp + j];
+                                const uint32_t hi = tag + 1 == nch ? qwin[j].y : cb[tag * qp + j];
+                                return make_uint2(lo, hi);
                             }
-                            const uint32_t incl = warp_incl_scan(cnt);
-                            if (j < qp) wpre[j] = carry + incl - cnt;
-                            carry += __shfl_sync(kFull, incl, 31);
-                        }
+                            const uint2 wj = qwin[j];
+                            const uint32_t lo = lower_bound_src(a.ent, wj.x, wj.y, ra);
+                            return make_uint2(lo, lower_bound_src(a.ent, lo, wj.y, rb));
+                        });
                         if (lane == 0) {
                             if (carry > Lay::cap && rb - ra > 1) {  // bisect; the lower half first
                                 const uint32_t mid = ra + (rb - ra) / 2;
@@ -428,7 +465,6 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                                 s_sp = sp + 1;
                                 s_L = kBisected;
                             } else {
-                                wpre[qp] = carry;
                                 s_sp = sp - 1;
                                 s_win += carry;
                                 s_L = carry;
@@ -446,29 +482,21 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
             while ((1u << hl) < 2 * L && hl < HLOG) hl++;
             const uint32_t mask = (1u << hl) - 1;
             // 1. accumulate: four entries' loads are issued before their slot updates.
-            uint32_t j = 0;
+            // Entries f0 + u NT + lane form one aligned group of 32 per warp.
             for (uint32_t f0 = tid - lane; f0 < L; f0 += 4 * NT) {
                 uint32_t sv[4], pv[4], jv[4];
 #pragma unroll
                 for (uint32_t u = 0; u < 4; u++) {
-                    const uint32_t f = f0 + lane + u * NT;
+                    const uint32_t g0 = f0 + u * NT, f = g0 + lane;
                     sv[u] = kEmpty;
                     if (f < L) {
-                        {   // the window holding entry f: the last j with wpre[j] <= f (a
-                            // binary search: its trip count is the same on every lane)
-                            uint32_t lo2 = 0, hi2 = qp;
-                            while (lo2 < hi2) {
-                                const uint32_t mid = (lo2 + hi2) >> 1;
-                                if (wpre[mid] <= f) lo2 = mid + 1;
-                                else hi2 = mid;
-                            }
-                            j = lo2 - 1;
-                        }
-                        const uint32_t k = clo[j] + (f - wpre[j]);
-                        const uint2 e = __ldg(a.ent + k);  // one 8-byte entry
+                        // the window of entry f: the last one starting at or below f
+                        const uint32_t g = g0 >> 5;
+                        const uint32_t r = gpre[g] + __popc(sbits[g] & (lanemask_lt() | (1u << lane))) - 1u;
+                        const uint2 e = __ldg(a.ent + (cbr[r] + f));  // one 8-byte entry
                         sv[u] = e.x;
                         pv[u] = e.y;  // source size << 16 | source position
-                        jv[u] = j;
+                        jv[u] = jr[r];
                     }
                 }
 #pragma unroll
