@@ -289,10 +289,12 @@ __device__ __forceinline__ void tally_overlap(const JoinArgs& a, FusedCounters& 
 // Per query: stage its tokens and membership structure, then per chunk of its
 // id window (one chunk when the windows fit the slot table):
 //   1. accumulate: every window entry (source s, query position j, source
-//      position and size from the index entry) goes into the shared slot table
-//      with one 64-bit CAS (key s; match count, last match positions); a
-//      newly occupied slot records the source's size beside it and is appended
-//      to the occupied list (one shared atomic per warp);
+//      position and size from the index entry; its window from the part's
+//      rank form) goes into the shared slot table, always used whole, with a
+//      read of its slot and one 64-bit CAS (key s; match count, last match
+//      positions); a newly occupied slot records the source's size beside it,
+//      and the slots a warp's four entry steps newly occupied go onto the
+//      occupied list with one shared atomic;
 //   2. decide: per occupied slot the reference-candidate and needs-merge tests
 //      read the slot word, the size beside it and the bound table (no gather
 //      per source); a slot that still needs a merge loads the source's bitmap
@@ -398,6 +400,17 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
         return carry;
     };
     if (one_chunk && wid == 0) lay_windows([&](uint32_t j) { return qwin[j]; });
+    if (!one_chunk) {
+        // the query's chunk boundaries and windows, into L2 ahead of its part setups
+        // (every address stays inside the two arrays)
+        const char* b0 = reinterpret_cast<const char*>(cb);
+        const uint32_t nb = (nch - 1) * qp * 4u;
+        for (uint32_t o = tid * 128u; o < nb; o += NT * 128u) asm volatile("prefetch.global.L2 [%0];" ::"l"(b0 + o));
+        if (tid == 0 && nb) asm volatile("prefetch.global.L2 [%0];" ::"l"(b0 + nb - 1));
+        const char* w0 = reinterpret_cast<const char*>(qwin);
+        for (uint32_t o = tid * 128u; o < qp * 8u; o += NT * 128u) asm volatile("prefetch.global.L2 [%0];" ::"l"(w0 + o));
+        if (tid == 0) asm volatile("prefetch.global.L2 [%0];" ::"l"(w0 + qp * 8u - 1));
+    }
     if (tid == 0) {
         s_cand = 0;
         s_win = 0;
@@ -478,13 +491,14 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                 if (L == kBisected) continue;
             }
             if (L == 0) continue;
-            int hl = 6;
-            while ((1u << hl) < 2 * L && hl < HLOG) hl++;
+            // the whole table for every part: the lowest load, so the shortest probe chains
+            const int hl = HLOG;
             const uint32_t mask = (1u << hl) - 1;
-            // 1. accumulate: four entries' loads are issued before their slot updates.
+            // 1. accumulate: four entries' loads are issued before their slot updates,
+            // and the slots they newly occupy go onto the occupied list together.
             // Entries f0 + u NT + lane form one aligned group of 32 per warp.
             for (uint32_t f0 = tid - lane; f0 < L; f0 += 4 * NT) {
-                uint32_t sv[4], pv[4], jv[4];
+                uint32_t sv[4], pv[4], jv[4], clm[4];
 #pragma unroll
                 for (uint32_t u = 0; u < 4; u++) {
                     const uint32_t g0 = f0 + u * NT, f = g0 + lane;
@@ -545,13 +559,25 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                             if (!done) atomicOr(a.status, ST_HASH_FULL);
                         }
                     }
-                    // newly occupied slots onto the occupied list, one shared atomic per warp
-                    const uint32_t m = __ballot_sync(kFull, claimed != 0xffffffffu);
-                    if (m) {
-                        uint32_t base = 0;
-                        if (lane == 0) base = atomicAdd(&s_nocc, (uint32_t)__popc(m));
-                        base = __shfl_sync(kFull, base, 0);
-                        if (claimed != 0xffffffffu) occ[base + __popc(m & lanemask_lt())] = (uint16_t)claimed;
+                    clm[u] = claimed;
+                }
+                // the slots the four steps newly occupied onto the occupied list, one shared
+                // atomic per warp
+                uint32_t mk[4], tot = 0;
+#pragma unroll
+                for (uint32_t u = 0; u < 4; u++) {
+                    mk[u] = __ballot_sync(kFull, clm[u] != 0xffffffffu);
+                    tot += __popc(mk[u]);
+                }
+                if (tot) {
+                    uint32_t base = 0;
+                    if (lane == 0) base = atomicAdd(&s_nocc, tot);
+                    base = __shfl_sync(kFull, base, 0);
+                    const uint32_t lt = lanemask_lt();
+#pragma unroll
+                    for (uint32_t u = 0; u < 4; u++) {
+                        if (clm[u] != 0xffffffffu) occ[base + __popc(mk[u] & lt)] = (uint16_t)clm[u];
+                        base += __popc(mk[u]);
                     }
                 }
             }
