@@ -14,7 +14,11 @@
  * larger set first.
  *
  * Ownership.  The caller owns its inputs.  The library owns what it returns
- * (fgss_sets, fgss_pairs) until the matching *_free call.
+ * (fgss_sets, fgss_pairs) until the matching *_free call.  The host columns
+ * of a result are one page-locked block where one can be had (the copies
+ * from the device run at the link's rate); fgss_pairs_free gives that block
+ * back to a process-wide pool, which keeps at most 1 GiB of free blocks for
+ * later results and releases the rest.
  *
  * Threading.  A context is bound to one device and one stream and is not
  * thread-safe; separate contexts are independent.
@@ -210,7 +214,7 @@ typedef struct fgss_pairs {
     /* candidates (want_candidates): (q, s, partial score) triples, host memory */
     uint32_t* cand;
     uint64_t n_cand;
-    void* priv;
+    void* priv;  /* the library's: the page-locked block holding the host columns, or NULL */
 } fgss_pairs;
 
 /* Self-join at one threshold; pairs sorted by (q, s).  Replaces

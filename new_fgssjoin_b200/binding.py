@@ -261,6 +261,21 @@ def ppjoin_format(path):
     return Sets.from_bin(path)
 
 
+class _PairsOwner:
+    """Owns one fgss_pairs result (a copy of the struct) and frees it once."""
+
+    def __init__(self, lib, p):
+        self._lib = lib
+        self._p = _Pairs()
+        ctypes.memmove(ctypes.byref(self._p), ctypes.byref(p), ctypes.sizeof(_Pairs))
+
+    def __del__(self):
+        try:
+            self._lib.fgss_pairs_free(ctypes.byref(self._p))
+        except Exception:  # interpreter shutdown
+            pass
+
+
 class Pairs:
     """Join result, sorted by (q, s): memory indices q < s, ids, overlap, sim."""
 
@@ -365,20 +380,26 @@ class Context:
         return o
 
     def _collect(self, p, st, want_candidates):
+        """Pairs over the library's host columns without copying them: the
+        columns are released (fgss_pairs_free) when the last array over them
+        is garbage-collected."""
         L = self._L
         n = p.n
+        owner = _PairsOwner(L, p)
 
-        def take(ptr, dtype=np.uint32):
-            return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype, copy=True) if n else np.zeros(0, dtype)
+        def take(ptr, ctype=ctypes.c_uint32, dtype=np.uint32):
+            if not n:
+                return np.zeros(0, dtype)
+            buf = (ctype * n).from_address(ctypes.cast(ptr, ctypes.c_void_p).value)
+            buf._owner = owner  # the arrays keep the columns alive
+            return np.frombuffer(buf, dtype)
         cands = None
         if want_candidates:
             nc = p.n_cand
             cands = (np.ctypeslib.as_array(p.cand, shape=(3 * nc,)).reshape(-1, 3).copy()
                      if nc else np.zeros((0, 3), np.uint32))
-        out = Pairs(take(p.q), take(p.s), take(p.id_q), take(p.id_s), take(p.overlap), take(p.sim, np.float32),
-                    _stats_dict(st), cands)
-        L.fgss_pairs_free(ctypes.byref(p))
-        return out
+        return Pairs(take(p.q), take(p.s), take(p.id_q), take(p.id_s), take(p.overlap),
+                     take(p.sim, ctypes.c_float, np.float32), _stats_dict(st), cands)
 
     def query_costs(self, sets, threshold, bounds="reference", use_model=True):
         """Per-query work estimates of the join (fgss_query_costs): window entries

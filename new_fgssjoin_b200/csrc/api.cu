@@ -72,8 +72,81 @@ void fill_stats(const JoinState& J, fgss_stats* st) {
     st->predicted_results = J.pred_results;
 }
 
-// Host columns of R pairs (freed by fgss_pairs_free).
+// Page-locked host blocks for the pairs handed to the caller: the device-to-host
+// copies of the columns run at the link's rate and write no freshly mapped
+// pages.  fgss_pairs_free gives a block back to a process-wide pool that the
+// next call takes it from; the pool keeps at most kPinnedPoolBytes of free
+// blocks and releases the rest.  Where page-locked memory cannot be had the
+// columns are malloc'd as before.
+struct PinnedPool {
+    std::mutex mu;
+    std::multimap<size_t, void*> free_blocks;  // size -> free block
+    std::map<void*, size_t> sizes;             // every block of the pool, handed out or free
+    size_t free_bytes = 0;
+};
+constexpr size_t kPinnedPoolBytes = size_t(1) << 30;
+
+PinnedPool& pinned_pool() {
+    static PinnedPool* pool = new PinnedPool;  // never destroyed: blocks may be given back at exit
+    return *pool;
+}
+
+// A block of at least `bytes` (a free one of at most twice the size, else a new
+// one), or nullptr.
+void* pinned_take(size_t bytes) {
+    PinnedPool& P = pinned_pool();
+    {
+        std::lock_guard<std::mutex> lk(P.mu);
+        auto it = P.free_blocks.lower_bound(bytes);
+        if (it != P.free_blocks.end() && it->first <= 2 * bytes + (size_t(1) << 20)) {
+            void* b = it->second;
+            P.free_bytes -= it->first;
+            P.free_blocks.erase(it);
+            return b;
+        }
+    }
+    void* b = nullptr;
+    if (cudaHostAlloc(&b, bytes, cudaHostAllocPortable) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(P.mu);
+    P.sizes[b] = bytes;
+    return b;
+}
+
+// Gives a block of the pool back (true), or returns false for other memory.
+bool pinned_give(void* b) {
+    PinnedPool& P = pinned_pool();
+    std::lock_guard<std::mutex> lk(P.mu);
+    auto it = P.sizes.find(b);
+    if (it == P.sizes.end()) return false;
+    const size_t sz = it->second;
+    if (P.free_bytes + sz <= kPinnedPoolBytes) {
+        P.free_blocks.emplace(sz, b);
+        P.free_bytes += sz;
+    } else {
+        P.sizes.erase(it);
+        if (cudaFreeHost(b) != cudaSuccess) (void)cudaGetLastError();
+    }
+    return true;
+}
+
+// Host columns of R pairs (freed by fgss_pairs_free): one page-locked block of
+// six 256-byte aligned columns (priv = the block), else six malloc'd columns.
 void alloc_host_pairs(fgss_pairs* out, uint64_t R) {
+    const size_t col = ((R ? R : 1) * 4 + 255) & ~size_t(255);
+    if (void* blk = pinned_take(6 * col)) {
+        char* b = static_cast<char*>(blk);
+        out->q = reinterpret_cast<uint32_t*>(b);
+        out->s = reinterpret_cast<uint32_t*>(b + col);
+        out->id_q = reinterpret_cast<uint32_t*>(b + 2 * col);
+        out->id_s = reinterpret_cast<uint32_t*>(b + 3 * col);
+        out->overlap = reinterpret_cast<uint32_t*>(b + 4 * col);
+        out->sim = reinterpret_cast<float*>(b + 5 * col);
+        out->priv = blk;
+        return;
+    }
     const size_t b = (R ? R : 1) * 4;
     out->q = (uint32_t*)malloc(b);
     out->s = (uint32_t*)malloc(b);
@@ -784,7 +857,9 @@ fgss_status fgss_selfjoin_batch(fgss_ctx* ctx, const fgss_sets_view* sets, const
 
 void fgss_pairs_free(fgss_pairs* p) {
     if (!p) return;
-    if (p->on_device) {
+    if (!p->on_device && p->priv && pinned_give(p->priv)) {
+        // the columns were one block of the page-locked pool
+    } else if (p->on_device) {
         cudaFree(p->q);
         cudaFree(p->s);
         cudaFree(p->id_q);
