@@ -33,8 +33,10 @@ constexpr uint32_t kSmaxUnknown = 2047;
 constexpr uint32_t kMemberBits = 14;
 constexpr uint32_t kMemberWords = 1u << (kMemberBits - 5);
 
-// Layout: slots u64[H] | occ u16[H] | sls u16[H] | cbr u32[PC] | jr u16[PC] |
-//         sbits u32[JW] | gpre u16[JW] | qtok u32[QC] | bm u32[BW] | mlist u16[MC]
+// Layout: slots u64[H] | occ u32[cap] | cbr u32[PC] | jr u16[PC] |
+//         sbits u32[JW] | gpre u16[JW] | qtok u32[QC] | bm u32[BW] | mlist u32[MC]
+// occ and mlist entries are slot | source size << 16 (a part's distinct sources
+// number at most cap).
 // The current part's windows are kept in rank form: its non-empty windows in
 // order get ranks r, cbr[r] = first entry - entries of the earlier windows
 // (so entry f of the part is ent[cbr[r] + f]) and jr[r] = the probe position;
@@ -48,9 +50,9 @@ struct FusedLayout {
     // probe tokens handled in shared memory: 256..384 (a slot's 11-bit query
     // position and 10-bit match count rely on PC <= 512); a query with more
     // goes to the global-memory accumulator.  The staging caps keep the
-    // 2^11-slot table at 31 KB, 7 CTAs of 128 threads per SM
+    // 2^11-slot layout at 30 KB, 7 CTAs of 128 threads per SM
     static constexpr uint32_t PC = H / 4 > 384 ? 384 : (H / 4 > 256 ? H / 4 : 256);
-    static constexpr uint32_t QC = H / 2 > 256 ? 256 : H / 2;  // query tokens staged in shared memory
+    static constexpr uint32_t QC = H / 2 > 512 ? 512 : H / 2;  // query tokens staged in shared memory
                                                                   // (longer: read from HBM)
     // entries of one part: at most cap, or PC when a part of one source id
     // (which holds at most one entry per probe window) cannot be bisected
@@ -60,15 +62,14 @@ struct FusedLayout {
     static constexpr uint32_t MC = 256;       // merge list entries per chunk (more: merged by their lane)
     static constexpr size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
     static constexpr size_t off_occ = 8ull * H;
-    static constexpr size_t off_sls = off_occ + 2ull * H;   // source size of each slot
-    static constexpr size_t off_cbr = off_sls + 2ull * H;
+    static constexpr size_t off_cbr = off_occ + 4ull * cap;
     static constexpr size_t off_jr = off_cbr + 4ull * PC;
     static constexpr size_t off_sbits = al16(off_jr + 2ull * PC);
     static constexpr size_t off_gpre = off_sbits + 4ull * JW;
     static constexpr size_t off_qtok = al16(off_gpre + 2ull * JW);
     static constexpr size_t off_bm = off_qtok + 4ull * QC;
     static constexpr size_t off_ml = off_bm + 4ull * BW;
-    static constexpr size_t bytes = off_ml + 2ull * MC;
+    static constexpr size_t bytes = off_ml + 4ull * MC;
     static_assert(off_bm % 16 == 0, "the membership words are cleared with 16-byte stores");
 };
 
@@ -310,15 +311,14 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
     using Lay = FusedLayout<HLOG>;
     constexpr uint32_t NW = NT / 32;
     unsigned long long* slots = reinterpret_cast<unsigned long long*>(smem);
-    uint16_t* occ = reinterpret_cast<uint16_t*>(smem + Lay::off_occ);
-    uint16_t* sls = reinterpret_cast<uint16_t*>(smem + Lay::off_sls);
+    uint32_t* occ = reinterpret_cast<uint32_t*>(smem + Lay::off_occ);
     uint32_t* cbr = reinterpret_cast<uint32_t*>(smem + Lay::off_cbr);
     uint16_t* jr = reinterpret_cast<uint16_t*>(smem + Lay::off_jr);
     uint32_t* sbits = reinterpret_cast<uint32_t*>(smem + Lay::off_sbits);
     uint16_t* gpre = reinterpret_cast<uint16_t*>(smem + Lay::off_gpre);
     uint32_t* qtok = reinterpret_cast<uint32_t*>(smem + Lay::off_qtok);
     uint32_t* bm = reinterpret_cast<uint32_t*>(smem + Lay::off_bm);
-    uint16_t* mlist = reinterpret_cast<uint16_t*>(smem + Lay::off_ml);
+    uint32_t* mlist = reinterpret_cast<uint32_t*>(smem + Lay::off_ml);
     __shared__ uint32_t s_sp, s_nocc, s_nm, s_cand, s_win, s_L;
     __shared__ uint4 s_qbm[4];  // the query's bitmap
     __shared__ uint32_t s_sa[48], s_sb[48], s_sc[48];
@@ -516,7 +516,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
 #pragma unroll
                 for (uint32_t u = 0; u < 4; u++) {
                     const uint32_t s = sv[u];
-                    uint32_t claimed = 0xffffffffu;  // the slot this entry newly occupied
+                    uint32_t claimed = 0xffffffffu;  // the slot this entry newly occupied | size << 16
                     if (s != kEmpty) {
                         const uint32_t ls = pv[u] >> 16;
                         bool skip = unsorted && !size_ok(a, lq, ls);
@@ -547,10 +547,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                                 }
                                 const unsigned long long prev = atomicCAS(&slots[h], old, nw);
                                 if (prev == old) {
-                                    if (key == kEmpty) {
-                                        claimed = h;
-                                        sls[h] = (uint16_t)ls;
-                                    }
+                                    if (key == kEmpty) claimed = h | (ls << 16);
                                     done = true;
                                 } else {
                                     old = prev;
@@ -576,7 +573,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                     const uint32_t lt = lanemask_lt();
 #pragma unroll
                     for (uint32_t u = 0; u < 4; u++) {
-                        if (clm[u] != 0xffffffffu) occ[base + __popc(mk[u] & lt)] = (uint16_t)clm[u];
+                        if (clm[u] != 0xffffffffu) occ[base + __popc(mk[u] & lt)] = clm[u];
                         base += __popc(mk[u]);
                     }
                 }
@@ -588,14 +585,14 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
             for (uint32_t i0 = tid - lane; i0 < nocc; i0 += NT) {
                 const uint32_t i = i0 + lane;
                 bool check = false;
-                uint32_t h = 0;
+                uint32_t e = 0;  // slot | source size << 16
                 if (i < nocc) {
-                    h = occ[i];
-                    const unsigned long long v = slots[h];
+                    e = occ[i];
+                    const uint32_t ls = e >> 16;
+                    const uint4 sm = __ldg(smin + ls);  // (cand_min, inter_min, need) of |q| + |s|
+                    const unsigned long long v = slots[e & 0xffffu];
                     const uint32_t s = (uint32_t)(v >> 32), lo = (uint32_t)v;
                     const uint32_t c = lo & 0x3ffu, jm = lo >> 21, smx = (lo >> 10) & 0x7ffu;
-                    const uint32_t ls = sls[h];
-                    const uint4 sm = __ldg(smin + ls);  // (cand_min, inter_min, need) of |q| + |s|
                     const uint32_t A = lq - jm;
                     bool cand, ver;
                     if (smx != kSmaxUnknown) {
@@ -634,13 +631,13 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
                     if (check) {
                         const uint32_t mi = base + __popc(m & lanemask_lt());
                         if (mi < Lay::MC) {
-                            mlist[mi] = (uint16_t)h;
+                            mlist[mi] = e;
                         } else {
                             // the merge list is full: this lane merges the source itself
-                            const unsigned long long v = slots[h];
+                            const unsigned long long v = slots[e & 0xffffu];
                             const uint32_t s = (uint32_t)(v >> 32), lo = (uint32_t)v;
                             const uint32_t c = lo & 0x3ffu, jm = lo >> 21, smx = (lo >> 10) & 0x7ffu;
-                            const uint32_t ls = sls[h];
+                            const uint32_t ls = e >> 16;
                             const uint4 sm = __ldg(smin + ls);
                             const uint32_t* st = a.tok + fa.meta[s].x;
                             const uint32_t xq = qsrc[jm], qrest = lq - jm - 1;
@@ -660,11 +657,11 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
             // 3. merge the listed sources (a warp per source) and clear the slots
             const uint32_t nm = min(s_nm, Lay::MC);
             for (uint32_t mi = wid; mi < nm; mi += NW) {
-                const uint32_t h = mlist[mi];
-                const unsigned long long v = slots[h];
+                const uint32_t e = mlist[mi];
+                const unsigned long long v = slots[e & 0xffffu];
                 const uint32_t s = (uint32_t)(v >> 32), lo = (uint32_t)v;
                 const uint32_t c = lo & 0x3ffu, jm = lo >> 21, smx = (lo >> 10) & 0x7ffu;
-                const uint32_t ls = sls[h];
+                const uint32_t ls = e >> 16;
                 const uint4 sm = __ldg(smin + ls);
                 const uint32_t im = sm.y;
                 const uint32_t* st = a.tok + fa.meta[s].x;
@@ -689,7 +686,7 @@ __device__ void fused_query(const JoinArgs& a, const FusedArgs& fa, uint32_t q, 
             __syncthreads();  // the merges read the slots
             // (the next barrier -- the next part's first, or the query's last -- orders
             // this clear before any later accumulate)
-            for (uint32_t i2 = tid; i2 < nocc; i2 += NT) slots[occ[i2]] = kEmptySlot;
+            for (uint32_t i2 = tid; i2 < nocc; i2 += NT) slots[occ[i2] & 0xffffu] = kEmptySlot;
             if (tid == 0) {
                 s_nocc = 0;
                 s_nm = 0;
