@@ -16,8 +16,8 @@
 //     shared memory; per chunk of its id window the window entries are
 //     accumulated into a shared-memory slot table (64-bit CAS per entry; the
 //     index entry carries the source's size), the occupied slots are decided
-//     from shared memory alone, the bitmap bound of the survivors is checked
-//     with a few lanes per source, and warps merge the few that remain.
+//     from shared memory and L1 alone, the deciding lane checks the bitmap
+//     bound of the survivors, and warps merge the few that remain.
 #pragma once
 
 #include "join_kernels.cuh"
