@@ -58,3 +58,12 @@ def test_strided_query_sample_covers_the_join():
     assert sum(p[1]["candidates"] for p in parts) == st["candidates"]
     got = np.sort(np.concatenate([p[0] for p in parts]), order=("q", "s"))
     assert np.array_equal(got["q"], full["q"]) and np.array_equal(got["s"], full["s"])
+
+
+def test_every_workload_has_a_profiled_dram_traffic():
+    """The roofline's `traffic` of every bench workload comes from its committed
+    ncu summary (profiles/k_fused_<workload>.md): both DRAM lines parse."""
+    import bench
+    for wl in ("heavy1m", "titles100k", "reads500k", "batch256", "rs200k", "titles18k", "heavy300k"):
+        t = bench.profiled_traffic(wl)
+        assert t is not None and t > 0, wl
